@@ -1,0 +1,156 @@
+"""ctypes binding of the C ABI declared in include/frforge_cuda.h.
+
+The shared library is built in-tree (``frforge_b200/libfrforge_cuda.so``).
+There is no fallback: if the library or a GPU is missing, every entry point
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfrforge_cuda.so")
+
+# status codes (frg_status)
+FRG_OK, FRG_DIVERGED, FRG_MAX_STEPS = 0, 1, 2
+FRG_ERR_INVALID_ARG, FRG_ERR_UNSUPPORTED_HOOK, FRG_ERR_OOM = -1, -2, -3
+FRG_ERR_CUDA, FRG_ERR_TIMEOUT, FRG_ERR_STATE = -4, -5, -6
+
+POINTS = {"gl": 0, "gll": 1}
+FLUX = {"rusanov": 0, "hllc": 1}
+TIME = {"ssp_rk3": 0, "ssp_rk2": 1}
+BC_KIND = {"periodic": 0, "transmissive": 1, "dirichlet": 2, "reflecting": 3, "xsplit": 4}
+METHOD = {"null": 0, "persson": 1}
+AV_FORM = {"conservative_br0": 0, "element_local_DD": 1}
+GEOM = {"affine": 0, "wavy": 1, "metrics": 2}
+STATUS_SYMBOL = {FRG_OK: "ok", FRG_DIVERGED: "diverged", FRG_MAX_STEPS: "max_steps"}
+
+_dp = C.POINTER(C.c_double)
+
+
+class frg_bc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("mode", C.c_int),
+        ("state", C.c_double * 4), ("state_b", C.c_double * 4),
+        ("x0", C.c_double), ("s0", C.c_double), ("s1", C.c_double), ("sdiv", C.c_double),
+    ]
+
+
+class frg_operators(C.Structure):
+    _fields_ = [
+        ("p", C.c_int), ("points", C.c_int),
+        ("xi", _dp), ("w", _dp), ("D", _dp), ("l_L", _dp), ("l_R", _dp),
+        ("gL_xi", _dp), ("gR_xi", _dp), ("V", _dp),
+    ]
+
+
+_METRIC_FIELDS = ["x_xi", "x_eta", "y_xi", "y_eta", "J",
+                  "nx_W", "ny_W", "sJ_W", "nx_E", "ny_E", "sJ_E",
+                  "nx_S", "ny_S", "sJ_S", "nx_N", "ny_N", "sJ_N", "h_char"]
+
+
+class frg_metrics2d(C.Structure):
+    _fields_ = [(n, _dp) for n in _METRIC_FIELDS]
+
+
+class frg_solve_desc(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("p", C.c_int), ("points", C.c_int), ("flux", C.c_int),
+        ("time_scheme", C.c_int), ("gamma", C.c_double),
+        ("nx", C.c_int), ("ny", C.c_int),
+        ("x_left", C.c_double), ("x_right", C.c_double),
+        ("y_bottom", C.c_double), ("y_top", C.c_double),
+        ("x_vertices", _dp), ("y_vertices", _dp),
+        ("bc", frg_bc * 4),
+        ("solid", C.c_void_p),
+        ("geometry", C.c_int), ("wavy_amp", C.c_double),
+        ("metrics", C.POINTER(frg_metrics2d)),
+        ("ops", C.POINTER(frg_operators)),
+        ("method", C.c_int), ("av_form", C.c_int),
+        ("kappa", C.c_double), ("s0_factor", C.c_double),
+        ("eps_floor", C.c_double), ("c_av", C.c_double),
+    ]
+
+
+class frg_result(C.Structure):
+    _fields_ = [("status", C.c_int), ("n_steps", C.c_int64), ("t", C.c_double)]
+
+
+class frg_solve_info(C.Structure):
+    _fields_ = [("ndof", C.c_size_t), ("nel", C.c_int), ("np", C.c_int), ("neq", C.c_int),
+                ("device_bytes", C.c_size_t), ("residual_evals", C.c_int64), ("steps", C.c_int64)]
+
+
+# Every symbol declared in include/frforge_cuda.h with its ctypes signature.
+SIGNATURES = {
+    "frg_abi_version": (C.c_int, []),
+    "frg_version": (C.c_char_p, []),
+    "frg_status_string": (C.c_char_p, [C.c_int]),
+    "frg_build_operators": (C.c_int, [C.c_int, C.c_int] + [_dp] * 10),
+    "frg_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "frg_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "frg_last_error": (C.c_char_p, [C.c_void_p]),
+    "frg_ctx_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "frg_solve_create": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(C.c_void_p)]),
+    "frg_solve_destroy": (C.c_int, [C.c_void_p]),
+    "frg_solve_get_info": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_info)]),
+    "frg_upload_state": (C.c_int, [C.c_void_p, _dp, C.c_size_t, C.c_double]),
+    "frg_download_state": (C.c_int, [C.c_void_p, _dp, C.c_size_t, C.POINTER(C.c_double)]),
+    "frg_residual": (C.c_int, [C.c_void_p, _dp, C.c_size_t]),
+    "frg_sense": (C.c_int, [C.c_void_p, _dp, C.c_size_t]),
+    "frg_compute_dt": (C.c_int, [C.c_void_p, C.c_double, _dp]),
+    "frg_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_int)]),
+    "frg_advance": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int64,
+                              C.POINTER(frg_result)]),
+    "frg_time_stages": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, _dp,
+                                  C.POINTER(frg_result)]),
+}
+
+_lib = None
+
+
+class FRGError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (frg status {code})")
+        self.code = code
+
+
+class UnsupportedHookError(FRGError):
+    """A capturing method overrides a hook that has no GPU implementation."""
+
+
+def load():
+    """Load libfrforge_cuda.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m frforge_b200.build` "
+                "(there is no CPU fallback)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(code: int, ctx=None, what: str = "") -> int:
+    if code < 0:
+        msg = what
+        if ctx:
+            err = load().frg_last_error(ctx)
+            if err:
+                msg = f"{what}: {err.decode()}"
+        if code == FRG_ERR_UNSUPPORTED_HOOK:
+            raise UnsupportedHookError(code, msg)
+        if code == FRG_ERR_INVALID_ARG:
+            raise ValueError(msg)
+        raise FRGError(code, msg)
+    return code
+
+
+def dptr(a):
+    return a.ctypes.data_as(_dp)

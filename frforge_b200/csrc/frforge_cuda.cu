@@ -1,0 +1,913 @@
+// C-ABI runtime of the B200 FR library: contexts, solves, state transfer,
+// residual / step / advance.  The time loop of integrate! runs on the device:
+// a one-thread control kernel computes dt (compute_dt) and clips the last step
+// (SSP_RK3.jl:185-189), the fused stage kernels advance the state, and an end
+// kernel books the step and the :ok / :diverged / :max_steps status.  Several
+// steps are captured into one CUDA graph; the host polls the status word
+// between graph launches.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "frg_device.cuh"
+#include "frg_internal.h"
+
+namespace frg {
+int launch_stage2d_np2(const Launch2D&, const StageBufs&, cudaStream_t);
+int launch_stage2d_np3(const Launch2D&, const StageBufs&, cudaStream_t);
+int launch_stage2d_np4(const Launch2D&, const StageBufs&, cudaStream_t);
+int launch_stage2d_np5(const Launch2D&, const StageBufs&, cudaStream_t);
+int launch_stage2d_np6(const Launch2D&, const StageBufs&, cudaStream_t);
+int launch_stage1d_np2(const Launch1D&, const StageBufs&, cudaStream_t);
+int launch_stage1d_np3(const Launch1D&, const StageBufs&, cudaStream_t);
+int launch_stage1d_np4(const Launch1D&, const StageBufs&, cudaStream_t);
+int launch_stage1d_np5(const Launch1D&, const StageBufs&, cudaStream_t);
+int launch_stage1d_np6(const Launch1D&, const StageBufs&, cudaStream_t);
+
+int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (L.ops->np) {
+    case 2: return launch_stage2d_np2(L, b, st);
+    case 3: return launch_stage2d_np3(L, b, st);
+    case 4: return launch_stage2d_np4(L, b, st);
+    case 5: return launch_stage2d_np5(L, b, st);
+    case 6: return launch_stage2d_np6(L, b, st);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream) {
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (L.ops->np) {
+    case 2: return launch_stage1d_np2(L, b, st);
+    case 3: return launch_stage1d_np3(L, b, st);
+    case 4: return launch_stage1d_np4(L, b, st);
+    case 5: return launch_stage1d_np5(L, b, st);
+    case 6: return launch_stage1d_np6(L, b, st);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+// ------------------------------------------------------------ control kernels
+
+// Top of the ssp_rk3!/ssp_rk2! loop body (SSP_RK3.jl:185-189): loop test,
+// dt from the CFL wave speed of the current state, last-step clipping.
+__global__ void step_begin_kernel(DevScalars* sc) {
+  if (sc->status != kRunning) {
+    sc->active = 0;
+    return;
+  }
+  if (!(sc->t < sc->t_final - 10 * kEps)) {
+    sc->status = kFinished;
+    sc->active = 0;
+    return;
+  }
+  double dt;
+  if (sc->fixed_dt > 0.0) {
+    dt = sc->fixed_dt;
+  } else {
+    double lam = __longlong_as_double((long long)sc->lam_bits);
+    lam = jmax(jmax(lam, kEps), kEps);
+    dt = sc->cfl * sc->hmin / ((double)sc->two_p1 * lam);
+  }
+  if (sc->t + dt > sc->t_final) dt = sc->t_final - sc->t;
+  sc->dt = dt;
+  sc->t0 = sc->t;
+  sc->flags = 0u;
+  sc->lam_bits = 0ull;
+  sc->active = 1;
+}
+
+// Bottom of the loop body: step count, status and the time of the state.
+__global__ void step_end_kernel(DevScalars* sc, int nstages) {
+  if (!sc->active) return;
+  sc->active = 0;
+  sc->n_steps += 1;
+  const unsigned f = sc->flags;
+  int div_stage = 0;
+  for (int s = 1; s <= nstages; ++s)
+    if (f & (1u << (2 * (s - 1)))) {
+      div_stage = s;
+      break;
+    }
+  if (!div_stage && (f & (2u << (2 * (nstages - 1))))) div_stage = 4;
+  const double t0 = sc->t0, dt = sc->dt;
+  sc->residual_evals += div_stage && div_stage <= nstages ? div_stage : nstages;
+  if (div_stage) {
+    sc->status = FRG_DIVERGED;
+    sc->diverged_stage = div_stage;
+    // state.t at the moment ssp_rk3_step! returned :diverged
+    if (div_stage == 1)
+      sc->t = t0;
+    else if (div_stage == 2 || div_stage == 4)
+      sc->t = t0 + dt;
+    else
+      sc->t = t0 + dt / 2.0;
+    return;
+  }
+  sc->t = t0 + dt;
+  if (sc->n_steps >= sc->max_steps) sc->status = FRG_MAX_STEPS;
+}
+
+}  // namespace frg
+
+using namespace frg;
+
+struct frg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+};
+
+struct frg_solve {
+  frg_ctx* ctx = nullptr;
+  int dim = 2, np = 0, nel = 0, neq = 4, nx = 0, ny = 1;
+  size_t ndof = 0;
+  int time_scheme = FRG_TIME_SSP_RK3;
+  int method = FRG_METHOD_NULL;
+  HostOps ops;
+  Launch2D L2{};
+  Launch1D L1{};
+  double* U[3] = {nullptr, nullptr, nullptr};
+  double* E[3] = {nullptr, nullptr, nullptr};
+  double* du = nullptr;
+  double* sigma = nullptr;
+  DevScalars* sc = nullptr;
+  DevScalars* hsc = nullptr;  // pinned host mirror
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  bool have_state = false;
+  int cur = 0;  // buffer index of the current state
+  double t = 0.0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  bool graph_lambda = false;
+  int64_t residual_evals = 0, steps = 0;
+  double hmin = 0.0;
+};
+
+namespace {
+
+int set_err(frg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_err(frg_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return FRG_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(c, FRG_ERR_OOM, m);
+  return set_err(c, FRG_ERR_CUDA, m);
+}
+
+#define FRG_CUDA(call, what)                          \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_err(s->ctx, e_, what); \
+  } while (0)
+
+template <class T>
+int dev_alloc(frg_solve* s, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 16);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "cudaMalloc");
+  s->allocs.push_back(q);
+  s->bytes += n * sizeof(T);
+  *p = (T*)q;
+  return FRG_OK;
+}
+
+template <class T>
+int dev_upload(frg_solve* s, T** p, const T* host, size_t n) {
+  int rc = dev_alloc(s, p, n);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(*p, host, n * sizeof(T), cudaMemcpyHostToDevice, s->ctx->stream);
+  return cuda_err(s->ctx, e, "upload");
+}
+
+BCDev to_dev(const frg_bc& b) {
+  BCDev d;
+  d.kind = b.kind;
+  d.mode = b.mode;
+  for (int c = 0; c < 4; ++c) {
+    d.st[c] = b.state[c];
+    d.stb[c] = b.state_b[c];
+  }
+  d.x0 = b.x0;
+  d.s0 = b.s0;
+  d.s1 = b.s1;
+  d.sdiv = b.sdiv == 0.0 ? 1.0 : b.sdiv;
+  return d;
+}
+
+int push_scalars(frg_solve* s) {
+  cudaError_t e = cudaMemcpyAsync(s->sc, s->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->ctx->stream);
+  return cuda_err(s->ctx, e, "scalars upload");
+}
+int pull_scalars(frg_solve* s) {
+  cudaError_t e = cudaMemcpyAsync(s->hsc, s->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
+  return cuda_err(s->ctx, e, "scalars download");
+}
+
+int launch(frg_solve* s, const StageBufs& b) {
+  int e = s->dim == 2 ? launch_stage2d(s->L2, b, s->ctx->stream) : launch_stage1d(s->L1, b, s->ctx->stream);
+  return e ? cuda_err(s->ctx, (cudaError_t)e, "stage kernel launch") : FRG_OK;
+}
+
+bool needs_eps(const frg_solve* s) { return s->method == FRG_METHOD_PERSSON; }
+
+// Element viscosity and wave speed of the state in buffer `buf` (prime mode).
+int prime(frg_solve* s, int buf, bool want_lambda) {
+  if (!needs_eps(s) && !want_lambda) return FRG_OK;
+  StageBufs b{};
+  b.us = s->U[buf];
+  b.eps_out = s->E[buf];
+  b.mode = kModePrime;
+  b.want_lambda = want_lambda;
+  b.sc = s->sc;
+  return launch(s, b);
+}
+
+// The kernels of one time step on the current stream (RK3: 3 stages).
+// With `ev` (an array of 2*nstages events) each stage kernel is bracketed by
+// events for profiling.
+int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
+  step_begin_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc);
+  const bool rk2 = s->time_scheme == FRG_TIME_SSP_RK2;
+  StageBufs b{};
+  b.use_sc = 1;
+  b.sc = s->sc;
+  b.mode = kModeStage;
+  b.rk2 = rk2;
+  // stage 1: u1 = u0 + dt L(u0)
+  b.stage = 1;
+  b.us = s->U[0];
+  b.u0 = s->U[0];
+  b.uout = s->U[1];
+  b.eps_in = s->E[0];
+  b.eps_out = s->E[1];
+  b.a = 1.0;
+  b.b = 0.0;
+  b.c = 1.0;
+  b.want_lambda = 0;
+  if (ev) cudaEventRecord(ev[0], s->ctx->stream);
+  int rc = launch(s, b);
+  if (ev) cudaEventRecord(ev[1], s->ctx->stream);
+  if (rc) return rc;
+  if (rk2) {
+    // u = 1/2 u0 + 1/2 u1 + 1/2 dt L(u1)  (SSP_RK2.jl:42-48)
+    b.stage = 2;
+    b.us = s->U[1];
+    b.u0 = s->U[0];
+    b.uout = s->U[0];
+    b.eps_in = s->E[1];
+    b.eps_out = s->E[0];
+    b.a = 1.0 / 2.0;
+    b.b = 1.0 / 2.0;
+    b.c = 1.0 / 2.0;
+    b.want_lambda = want_lambda;
+    if (ev) cudaEventRecord(ev[2], s->ctx->stream);
+    rc = launch(s, b);
+    if (ev) cudaEventRecord(ev[3], s->ctx->stream);
+    if (rc) return rc;
+  } else {
+    // u2 = 3/4 u0 + 1/4 u1 + 1/4 dt L(u1)
+    b.stage = 2;
+    b.us = s->U[1];
+    b.u0 = s->U[0];
+    b.uout = s->U[2];
+    b.eps_in = s->E[1];
+    b.eps_out = s->E[2];
+    b.a = 3.0 / 4.0;
+    b.b = 1.0 / 4.0;
+    b.c = 1.0 / 4.0;
+    if (ev) cudaEventRecord(ev[2], s->ctx->stream);
+    rc = launch(s, b);
+    if (ev) cudaEventRecord(ev[3], s->ctx->stream);
+    if (rc) return rc;
+    // u = 1/3 u0 + 2/3 u2 + 2/3 dt L(u2)
+    b.stage = 3;
+    b.us = s->U[2];
+    b.u0 = s->U[0];
+    b.uout = s->U[0];
+    b.eps_in = s->E[2];
+    b.eps_out = s->E[0];
+    b.a = 1.0 / 3.0;
+    b.b = 2.0 / 3.0;
+    b.c = 2.0 / 3.0;
+    b.want_lambda = want_lambda;
+    if (ev) cudaEventRecord(ev[4], s->ctx->stream);
+    rc = launch(s, b);
+    if (ev) cudaEventRecord(ev[5], s->ctx->stream);
+    if (rc) return rc;
+  }
+  step_end_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc, rk2 ? 2 : 3);
+  cudaError_t e = cudaGetLastError();
+  return cuda_err(s->ctx, e, "control kernel");
+}
+
+// Copy buffer `src` into the canonical state buffer 0 after a divergence.
+int make_current_canonical(frg_solve* s) {
+  if (s->cur == 0) return FRG_OK;
+  FRG_CUDA(cudaMemcpyAsync(s->U[0], s->U[s->cur], s->ndof * sizeof(double), cudaMemcpyDeviceToDevice,
+                           s->ctx->stream),
+           "state copy");
+  s->cur = 0;
+  return FRG_OK;
+}
+
+int finish_run(frg_solve* s) {
+  int rc = pull_scalars(s);
+  if (rc) return rc;
+  s->t = s->hsc->t;
+  s->steps = s->hsc->n_steps;
+  s->residual_evals = s->hsc->residual_evals;
+  if (s->hsc->status == FRG_DIVERGED) {
+    const int ds = s->hsc->diverged_stage;
+    s->cur = (ds == 4 || ds == 1) ? 0 : (ds == 2 ? 1 : 2);
+    rc = make_current_canonical(s);
+    if (rc) return rc;
+  }
+  return FRG_OK;
+}
+
+int validate(frg_ctx* c, const frg_solve_desc* d) {
+  if (!d) return set_err(c, FRG_ERR_INVALID_ARG, "null descriptor");
+  if (d->dim != 1 && d->dim != 2) return set_err(c, FRG_ERR_INVALID_ARG, "dim must be 1 or 2");
+  if (d->p < 1 || d->p > FRG_MAX_NP - 1) return set_err(c, FRG_ERR_INVALID_ARG, "p must be in 1..5");
+  if (d->points != FRG_POINTS_GL && d->points != FRG_POINTS_GLL)
+    return set_err(c, FRG_ERR_INVALID_ARG, "points must be :gl or :gll");
+  if (d->flux != FRG_FLUX_RUSANOV && d->flux != FRG_FLUX_HLLC)
+    return set_err(c, FRG_ERR_INVALID_ARG, "flux must be :rusanov or :hllc");
+  if (d->time_scheme != FRG_TIME_SSP_RK3 && d->time_scheme != FRG_TIME_SSP_RK2)
+    return set_err(c, FRG_ERR_INVALID_ARG, "time must be :ssp_rk3 or :ssp_rk2");
+  if (d->nx < 1 || (d->dim == 2 && d->ny < 1)) return set_err(c, FRG_ERR_INVALID_ARG, "n_elements must be >= 1");
+  if (!d->x_vertices && !(d->x_right > d->x_left)) return set_err(c, FRG_ERR_INVALID_ARG, "x_right must be > x_left");
+  if (d->dim == 2 && !d->y_vertices && !(d->y_top > d->y_bottom))
+    return set_err(c, FRG_ERR_INVALID_ARG, "y_top > y_bottom required");
+  const int nb = d->dim == 1 ? 2 : 4;
+  for (int k = 0; k < nb; ++k) {
+    const int kind = d->bc[k].kind;
+    if (kind < FRG_BC_PERIODIC || kind > FRG_BC_XSPLIT) return set_err(c, FRG_ERR_INVALID_ARG, "unknown BC kind");
+    if (d->dim == 1 && (kind == FRG_BC_REFLECTING || kind == FRG_BC_XSPLIT))
+      return set_err(c, FRG_ERR_UNSUPPORTED_HOOK, "1D residual supports periodic/transmissive/Dirichlet ends");
+  }
+  if ((d->bc[0].kind == FRG_BC_PERIODIC) != (d->bc[1].kind == FRG_BC_PERIODIC))
+    return set_err(c, FRG_ERR_INVALID_ARG, "Periodic BC must be set on both ends");
+  if (d->dim == 2 && (d->bc[2].kind == FRG_BC_PERIODIC) != (d->bc[3].kind == FRG_BC_PERIODIC))
+    return set_err(c, FRG_ERR_INVALID_ARG, "y-periodic requires both bottom and top PeriodicBC");
+  if (d->method != FRG_METHOD_NULL && d->method != FRG_METHOD_PERSSON)
+    return set_err(c, FRG_ERR_UNSUPPORTED_HOOK, "capturing method has no GPU implementation");
+  if (d->method == FRG_METHOD_PERSSON && d->av_form != FRG_AV_BR0 && d->av_form != FRG_AV_LOCAL_DD)
+    return set_err(c, FRG_ERR_INVALID_ARG, "Unsupported av_form");
+  if (d->dim == 2 && d->geometry == FRG_GEOM_METRICS && !d->metrics)
+    return set_err(c, FRG_ERR_INVALID_ARG, "FRG_GEOM_METRICS needs metrics");
+  if (d->dim == 1 && d->solid) return set_err(c, FRG_ERR_INVALID_ARG, "solid masks are 2D only");
+  return FRG_OK;
+}
+
+// analytic wavy map partials, MeshMetrics2D.jl:310-318
+void wavy_partials(double X, double Y, double a, double* xX, double* xY, double* yX, double* yY) {
+  const double tp = 6.283185307179586, pi = 3.141592653589793;
+  *xX = 1.0 + a * std::sin(tp * Y) * pi * std::cos(pi * X);
+  *xY = a * tp * std::cos(tp * Y) * std::sin(pi * X);
+  *yX = a * tp * std::cos(tp * X) * std::sin(pi * Y);
+  *yY = 1.0 + a * std::sin(tp * X) * pi * std::cos(pi * Y);
+}
+
+int setup_2d(frg_solve* s, const frg_solve_desc* d) {
+  const int nx = d->nx, ny = d->ny, np = s->np, nel = nx * ny;
+  std::vector<double> xv(nx + 1), yv(ny + 1);
+  if (d->x_vertices)
+    std::memcpy(xv.data(), d->x_vertices, sizeof(double) * (nx + 1));
+  else
+    julia_linspace(d->x_left, d->x_right, nx + 1, xv.data());
+  if (d->y_vertices)
+    std::memcpy(yv.data(), d->y_vertices, sizeof(double) * (ny + 1));
+  else
+    julia_linspace(d->y_bottom, d->y_top, ny + 1, yv.data());
+  std::vector<double> xc(nx), Jx(nx), dx(nx), yc(ny), Jy(ny), dy(ny), hchar(nel);
+  for (int i = 0; i < nx; ++i) {
+    xc[i] = (xv[i] + xv[i + 1]) / 2.0;
+    dx[i] = xv[i + 1] - xv[i];
+    Jx[i] = dx[i] / 2.0;
+  }
+  for (int i = 0; i < ny; ++i) {
+    yc[i] = (yv[i] + yv[i + 1]) / 2.0;
+    dy[i] = yv[i + 1] - yv[i];
+    Jy[i] = dy[i] / 2.0;
+  }
+  for (int e = 0; e < nel; ++e) hchar[e] = std::fmin(dx[e % nx], dy[e / nx]);
+  Mesh2Dev& M = s->L2.mesh;
+  std::memset(&M, 0, sizeof(M));
+  M.nx = nx;
+  M.ny = ny;
+  M.nel = nel;
+  M.px = d->bc[0].kind == FRG_BC_PERIODIC;
+  M.py = d->bc[2].kind == FRG_BC_PERIODIC;
+  for (int k = 0; k < 4; ++k) M.bc[k] = to_dev(d->bc[k]);
+  M.wavy = d->geometry == FRG_GEOM_WAVY;
+  M.amp = d->wavy_amp;
+  int rc;
+  double* p;
+  if ((rc = dev_upload(s, &p, xc.data(), nx))) return rc;
+  M.xc = p;
+  if ((rc = dev_upload(s, &p, Jx.data(), nx))) return rc;
+  M.Jx = p;
+  if ((rc = dev_upload(s, &p, dx.data(), nx))) return rc;
+  M.dx = p;
+  if ((rc = dev_upload(s, &p, yc.data(), ny))) return rc;
+  M.yc = p;
+  if ((rc = dev_upload(s, &p, Jy.data(), ny))) return rc;
+  M.Jy = p;
+  if ((rc = dev_upload(s, &p, dy.data(), ny))) return rc;
+  M.dy = p;
+  if (d->solid) {
+    unsigned char* q;
+    if ((rc = dev_upload(s, &q, d->solid, (size_t)nel))) return rc;
+    M.solid = q;
+  }
+  if (d->geometry == FRG_GEOM_AFFINE) {
+    if ((rc = dev_upload(s, &p, hchar.data(), nel))) return rc;
+    M.hchar = p;
+    s->hmin = hchar[0];
+    for (int e = 1; e < nel; ++e) s->hmin = std::fmin(s->hmin, hchar[e]);
+    return FRG_OK;
+  }
+  // curved: per-SP metric fields (element-major [e][k]) and face normals
+  M.curved = 1;
+  const size_t nsp = (size_t)nel * np * np, nfp = (size_t)nel * np;
+  std::vector<double> xxi(nsp), xeta(nsp), yxi(nsp), yeta(nsp), rJ(nsp);
+  std::vector<double> fn[3][4];
+  for (int a = 0; a < 3; ++a)
+    for (int f = 0; f < 4; ++f) fn[a][f].resize(nfp);
+  if (d->geometry == FRG_GEOM_WAVY) {
+    // build_mesh_metrics_analytic_wavy, MeshMetrics2D.jl:327-442
+    const double amp = d->wavy_amp;
+    for (int e = 0; e < nel; ++e) {
+      const int jx = e % nx, jy = e / nx;
+      for (int j = 0; j < np; ++j)
+        for (int i = 0; i < np; ++i) {
+          const double X = xc[jx] + Jx[jx] * s->ops.xi[i], Y = yc[jy] + Jy[jy] * s->ops.xi[j];
+          double a, b, c2, d2;
+          wavy_partials(X, Y, amp, &a, &b, &c2, &d2);
+          const size_t k = (size_t)e * np * np + i + np * j;
+          xxi[k] = a * Jx[jx];
+          xeta[k] = b * Jy[jy];
+          yxi[k] = c2 * Jx[jx];
+          yeta[k] = d2 * Jy[jy];
+          rJ[k] = 1.0 / (xxi[k] * yeta[k] - xeta[k] * yxi[k]);
+        }
+      for (int q = 0; q < np; ++q) {
+        const size_t k = (size_t)e * np + q;
+        const double Y = yc[jy] + Jy[jy] * s->ops.xi[q], X = xc[jx] + Jx[jx] * s->ops.xi[q];
+        double a, b, c2, d2;
+        // west / east: n ~ (-y_eta, x_eta) / (y_eta, -x_eta)
+        for (int side = 0; side < 2; ++side) {
+          wavy_partials(xc[jx] + Jx[jx] * (side ? 1.0 : -1.0), Y, amp, &a, &b, &c2, &d2);
+          const double xe = b * Jy[jy], ye = d2 * Jy[jy];
+          const double sJ = std::fmax(std::sqrt(ye * ye + xe * xe), kEps);
+          fn[0][side][k] = side ? ye / sJ : -ye / sJ;
+          fn[1][side][k] = side ? -xe / sJ : xe / sJ;
+          fn[2][side][k] = sJ;
+        }
+        // south / north: n ~ (y_xi, -x_xi) / (-y_xi, x_xi)
+        for (int side = 0; side < 2; ++side) {
+          wavy_partials(X, yc[jy] + Jy[jy] * (side ? 1.0 : -1.0), amp, &a, &b, &c2, &d2);
+          const double xx = a * Jx[jx], yx = c2 * Jx[jx];
+          const double sJ = std::fmax(std::sqrt(yx * yx + xx * xx), kEps);
+          fn[0][2 + side][k] = side ? -yx / sJ : yx / sJ;
+          fn[1][2 + side][k] = side ? xx / sJ : -xx / sJ;
+          fn[2][2 + side][k] = sJ;
+        }
+      }
+    }
+  } else {
+    const frg_metrics2d* m = d->metrics;
+    const double* srcf[3][4] = {{m->nx_W, m->nx_E, m->nx_S, m->nx_N},
+                                {m->ny_W, m->ny_E, m->ny_S, m->ny_N},
+                                {m->sJ_W, m->sJ_E, m->sJ_S, m->sJ_N}};
+    for (size_t k = 0; k < nsp; ++k) {
+      xxi[k] = m->x_xi[k];
+      xeta[k] = m->x_eta[k];
+      yxi[k] = m->y_xi[k];
+      yeta[k] = m->y_eta[k];
+      rJ[k] = 1.0 / m->J[k];
+    }
+    for (int a = 0; a < 3; ++a)
+      for (int f = 0; f < 4; ++f) std::memcpy(fn[a][f].data(), srcf[a][f], nfp * sizeof(double));
+    if (m->h_char) std::memcpy(hchar.data(), m->h_char, nel * sizeof(double));
+  }
+  if ((rc = dev_upload(s, &p, hchar.data(), nel))) return rc;
+  M.hchar = p;
+  s->hmin = hchar[0];
+  for (int e = 1; e < nel; ++e) s->hmin = std::fmin(s->hmin, hchar[e]);
+  if ((rc = dev_upload(s, &p, xxi.data(), nsp))) return rc;
+  M.m_xxi = p;
+  if ((rc = dev_upload(s, &p, xeta.data(), nsp))) return rc;
+  M.m_xeta = p;
+  if ((rc = dev_upload(s, &p, yxi.data(), nsp))) return rc;
+  M.m_yxi = p;
+  if ((rc = dev_upload(s, &p, yeta.data(), nsp))) return rc;
+  M.m_yeta = p;
+  if ((rc = dev_upload(s, &p, rJ.data(), nsp))) return rc;
+  M.m_rJ = p;
+  for (int f = 0; f < 4; ++f) {
+    if ((rc = dev_upload(s, &p, fn[0][f].data(), nfp))) return rc;
+    M.f_nx[f] = p;
+    if ((rc = dev_upload(s, &p, fn[1][f].data(), nfp))) return rc;
+    M.f_ny[f] = p;
+    if ((rc = dev_upload(s, &p, fn[2][f].data(), nfp))) return rc;
+    M.f_sJ[f] = p;
+  }
+  return FRG_OK;
+}
+
+int setup_1d(frg_solve* s, const frg_solve_desc* d) {
+  const int nel = d->nx;
+  std::vector<double> xv(nel + 1), xc(nel), J(nel), dx(nel);
+  if (d->x_vertices)
+    std::memcpy(xv.data(), d->x_vertices, sizeof(double) * (nel + 1));
+  else
+    julia_linspace(d->x_left, d->x_right, nel + 1, xv.data());
+  s->hmin = INFINITY;
+  for (int e = 0; e < nel; ++e) {
+    dx[e] = xv[e + 1] - xv[e];
+    J[e] = dx[e] / 2.0;
+    xc[e] = (xv[e] + xv[e + 1]) / 2.0;
+    s->hmin = std::fmin(s->hmin, dx[e]);
+  }
+  Mesh1Dev& M = s->L1.mesh;
+  std::memset(&M, 0, sizeof(M));
+  M.nel = nel;
+  M.periodic = d->bc[0].kind == FRG_BC_PERIODIC;
+  M.bc[0] = to_dev(d->bc[0]);
+  M.bc[1] = to_dev(d->bc[1]);
+  int rc;
+  double* p;
+  if ((rc = dev_upload(s, &p, xc.data(), nel))) return rc;
+  M.xc = p;
+  if ((rc = dev_upload(s, &p, J.data(), nel))) return rc;
+  M.J = p;
+  if ((rc = dev_upload(s, &p, dx.data(), nel))) return rc;
+  M.dx = p;
+  return FRG_OK;
+}
+
+void release(frg_solve* s) {
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->hsc) cudaFreeHost(s->hsc);
+  s->allocs.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+int frg_abi_version(void) { return FRG_ABI_VERSION; }
+const char* frg_version(void) { return "frforge_b200 0.1 (sm_100a, FP64)"; }
+
+const char* frg_status_string(int st) {
+  switch (st) {
+    case FRG_OK: return "ok";
+    case FRG_DIVERGED: return "diverged";
+    case FRG_MAX_STEPS: return "max_steps";
+    case FRG_ERR_INVALID_ARG: return "invalid argument";
+    case FRG_ERR_UNSUPPORTED_HOOK: return "unsupported hook";
+    case FRG_ERR_OOM: return "out of device memory";
+    case FRG_ERR_CUDA: return "CUDA error";
+    case FRG_ERR_TIMEOUT: return "timeout";
+    case FRG_ERR_STATE: return "invalid call order";
+  }
+  return "unknown status";
+}
+
+int frg_ctx_create(int device, frg_ctx** out) {
+  if (!out) return FRG_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return FRG_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return FRG_ERR_CUDA;
+  frg_ctx* c = new (std::nothrow) frg_ctx();
+  if (!c) return FRG_ERR_OOM;
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return FRG_ERR_CUDA;
+  }
+  *out = c;
+  return FRG_OK;
+}
+
+int frg_ctx_destroy(frg_ctx* c) {
+  if (!c) return FRG_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return FRG_OK;
+}
+
+const char* frg_last_error(const frg_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int frg_ctx_get_stream(frg_ctx* c, void** stream) {
+  if (!c || !stream) return FRG_ERR_INVALID_ARG;
+  *stream = (void*)c->stream;
+  return FRG_OK;
+}
+
+int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
+  if (!c || !out) return FRG_ERR_INVALID_ARG;
+  *out = nullptr;
+  int rc = validate(c, d);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  frg_solve* s = new (std::nothrow) frg_solve();
+  if (!s) return set_err(c, FRG_ERR_OOM, "host allocation");
+  s->ctx = c;
+  s->dim = d->dim;
+  s->np = d->p + 1;
+  s->neq = d->dim == 1 ? 3 : 4;
+  s->nx = d->nx;
+  s->ny = d->dim == 1 ? 1 : d->ny;
+  s->nel = s->nx * s->ny;
+  s->ndof = (size_t)s->nel * (d->dim == 1 ? s->np : s->np * s->np) * s->neq;
+  s->time_scheme = d->time_scheme;
+  s->method = d->method;
+  rc = d->ops ? host_ops_from_caller(d->ops, &s->ops) : build_host_ops(d->p, d->points, &s->ops);
+  if (rc) {
+    delete s;
+    return set_err(c, rc, "operator tables");
+  }
+  Phys P;
+  P.gamma = d->gamma;
+  P.g1 = d->gamma - 1.0;
+  P.c_av = d->c_av;
+  P.kappa = d->kappa;
+  P.eps_floor = d->eps_floor;
+  P.p = d->p;
+  P.pm = d->p > 1 ? d->p : 1;
+  P.s0 = d->s0_factor * std::log10((double)P.pm);  // persson_s0, SharedAV.jl:9-11
+  const int av = d->method == FRG_METHOD_PERSSON ? (d->av_form == FRG_AV_LOCAL_DD ? kAvDD : kAvBR0) : kAvNone;
+  rc = d->dim == 2 ? setup_2d(s, d) : setup_1d(s, d);
+  if (!rc) {
+    s->L2.ops = &s->ops;
+    s->L2.phys = P;
+    s->L2.flux = d->flux;
+    s->L2.av = av;
+    s->L1.ops = &s->ops;
+    s->L1.phys = P;
+    s->L1.flux = d->flux;
+    s->L1.av = av;
+    for (int k = 0; k < 3 && !rc; ++k) rc = dev_alloc(s, &s->U[k], s->ndof);
+    for (int k = 0; k < 3 && !rc; ++k) rc = dev_alloc(s, &s->E[k], (size_t)s->nel);
+    if (!rc) rc = dev_alloc(s, &s->sc, 1);
+  }
+  if (!rc) {
+    if (cudaMallocHost(&s->hsc, sizeof(DevScalars)) != cudaSuccess) rc = set_err(c, FRG_ERR_OOM, "pinned scalars");
+  }
+  if (!rc) {
+    std::memset(s->hsc, 0, sizeof(DevScalars));
+    s->hsc->two_p1 = 2 * d->p + 1;
+    s->hsc->hmin = s->hmin;
+    for (int k = 0; k < 3 && !rc; ++k)
+      rc = cuda_err(c, cudaMemsetAsync(s->E[k], 0, sizeof(double) * s->nel, c->stream), "memset");
+    if (!rc) rc = push_scalars(s);
+    if (!rc) rc = cuda_err(c, cudaStreamSynchronize(c->stream), "solve setup");
+  }
+  if (rc) {
+    release(s);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return FRG_OK;
+}
+
+int frg_solve_destroy(frg_solve* s) {
+  if (!s) return FRG_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  release(s);
+  delete s;
+  return FRG_OK;
+}
+
+int frg_solve_get_info(const frg_solve* s, frg_solve_info* info) {
+  if (!s || !info) return FRG_ERR_INVALID_ARG;
+  info->ndof = s->ndof;
+  info->nel = s->nel;
+  info->np = s->np;
+  info->neq = s->neq;
+  info->device_bytes = s->bytes;
+  info->residual_evals = s->residual_evals;
+  info->steps = s->steps;
+  return FRG_OK;
+}
+
+int frg_upload_state(frg_solve* s, const double* u, size_t n, double t) {
+  if (!s || !u) return FRG_ERR_INVALID_ARG;
+  if (n != s->ndof) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "state length mismatch");
+  cudaSetDevice(s->ctx->device);
+  FRG_CUDA(cudaMemcpyAsync(s->U[0], u, n * sizeof(double), cudaMemcpyHostToDevice, s->ctx->stream), "upload");
+  s->t = t;
+  s->cur = 0;
+  s->have_state = true;
+  s->hsc->t = t;
+  return push_scalars(s);
+}
+
+int frg_download_state(frg_solve* s, double* u, size_t n, double* t) {
+  if (!s || !u) return FRG_ERR_INVALID_ARG;
+  if (n != s->ndof) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "state length mismatch");
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  cudaSetDevice(s->ctx->device);
+  FRG_CUDA(cudaMemcpyAsync(u, s->U[s->cur], n * sizeof(double), cudaMemcpyDeviceToHost, s->ctx->stream),
+           "download");
+  FRG_CUDA(cudaStreamSynchronize(s->ctx->stream), "download sync");
+  if (t) *t = s->t;
+  return FRG_OK;
+}
+
+int frg_residual(frg_solve* s, double* du, size_t n) {
+  if (!s || !du) return FRG_ERR_INVALID_ARG;
+  if (n != s->ndof) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "du length mismatch");
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  cudaSetDevice(s->ctx->device);
+  int rc;
+  if (!s->du && (rc = dev_alloc(s, &s->du, s->ndof))) return rc;
+  s->hsc->t = s->t;
+  s->hsc->dt = 0.0;
+  if ((rc = push_scalars(s))) return rc;
+  if ((rc = prime(s, s->cur, false))) return rc;
+  StageBufs b{};
+  b.us = s->U[s->cur];
+  b.eps_in = s->E[s->cur];
+  b.du_out = s->du;
+  b.mode = kModeResidual;
+  b.stage = 1;
+  b.sc = s->sc;
+  if ((rc = launch(s, b))) return rc;
+  FRG_CUDA(cudaMemcpyAsync(du, s->du, n * sizeof(double), cudaMemcpyDeviceToHost, s->ctx->stream), "du download");
+  FRG_CUDA(cudaStreamSynchronize(s->ctx->stream), "residual");
+  s->residual_evals += 1;
+  return FRG_OK;
+}
+
+int frg_sense(frg_solve* s, double* sigma, size_t nel) {
+  if (!s || !sigma) return FRG_ERR_INVALID_ARG;
+  if (nel != (size_t)s->nel) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "sigma length mismatch");
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  if (s->method != FRG_METHOD_PERSSON) {
+    for (size_t e = 0; e < nel; ++e) sigma[e] = 0.0;  // NullSensor (Interfaces.jl:101-104)
+    return FRG_OK;
+  }
+  cudaSetDevice(s->ctx->device);
+  int rc;
+  if (!s->sigma && (rc = dev_alloc(s, &s->sigma, (size_t)s->nel))) return rc;
+  StageBufs b{};
+  b.us = s->U[s->cur];
+  b.sigma_out = s->sigma;
+  b.mode = kModeSense;
+  b.sc = s->sc;
+  if ((rc = launch(s, b))) return rc;
+  FRG_CUDA(cudaMemcpyAsync(sigma, s->sigma, nel * sizeof(double), cudaMemcpyDeviceToHost, s->ctx->stream),
+           "sigma download");
+  FRG_CUDA(cudaStreamSynchronize(s->ctx->stream), "sense");
+  return FRG_OK;
+}
+
+int frg_compute_dt(frg_solve* s, double cfl, double* dt) {
+  if (!s || !dt) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  cudaSetDevice(s->ctx->device);
+  int rc;
+  s->hsc->lam_bits = 0ull;
+  if ((rc = push_scalars(s))) return rc;
+  if ((rc = prime(s, s->cur, true))) return rc;
+  if ((rc = pull_scalars(s))) return rc;
+  double lam;
+  std::memcpy(&lam, &s->hsc->lam_bits, sizeof(lam));
+  lam = std::fmax(std::fmax(lam, kEps), kEps);
+  if (std::isnan(lam)) lam = NAN;
+  *dt = cfl * s->hmin / ((double)(2 * (s->np - 1) + 1) * lam);
+  return FRG_OK;
+}
+
+static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps,
+                     frg_result* out, bool use_graph, double* stage_ms = nullptr) {
+  cudaSetDevice(s->ctx->device);
+  int rc = make_current_canonical(s);
+  if (rc) return rc;
+  const bool want_lambda = !(fixed_dt > 0.0);
+  DevScalars& h = *s->hsc;
+  h.t = s->t;
+  h.t_final = t_final;
+  h.cfl = cfl;
+  h.fixed_dt = fixed_dt;
+  h.hmin = s->hmin;
+  h.two_p1 = 2 * (s->np - 1) + 1;
+  h.status = kRunning;
+  h.active = 0;
+  h.flags = 0;
+  h.diverged_stage = 0;
+  h.lam_bits = 0ull;
+  h.n_steps = 0;
+  h.max_steps = max_steps;
+  h.residual_evals = s->residual_evals;
+  if ((rc = push_scalars(s))) return rc;
+  if ((rc = prime(s, 0, want_lambda))) return rc;
+  // steps per graph: keep one graph launch around a few milliseconds of work
+  const double dof_per_step = (double)s->ndof;
+  int K = dof_per_step > 4e6 ? 4 : (dof_per_step > 2e5 ? 16 : 64);
+  if (!use_graph) K = 1;
+  if (use_graph) {
+    // the graph depends only on buffers, tables and the dt mode of the solve
+    if (!s->graph || s->graph_steps != K || s->graph_lambda != want_lambda) {
+      if (s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+      }
+      cudaGraph_t g;
+      FRG_CUDA(cudaStreamBeginCapture(s->ctx->stream, cudaStreamCaptureModeThreadLocal), "capture begin");
+      int crc = FRG_OK;
+      for (int k = 0; k < K && !crc; ++k) crc = enqueue_step(s, want_lambda);
+      cudaError_t ce = cudaStreamEndCapture(s->ctx->stream, &g);
+      if (crc) return crc;
+      FRG_CUDA(ce, "capture end");
+      ce = cudaGraphInstantiate(&s->graph, g, 0);
+      cudaGraphDestroy(g);
+      FRG_CUDA(ce, "graph instantiate");
+      s->graph_steps = K;
+      s->graph_lambda = want_lambda;
+    }
+  }
+  cudaEvent_t ev[6];
+  double acc[3] = {0.0, 0.0, 0.0};
+  int64_t nt = 0;
+  if (stage_ms)
+    for (int k = 0; k < 6; ++k) cudaEventCreate(&ev[k]);
+  for (;;) {
+    if (use_graph) {
+      FRG_CUDA(cudaGraphLaunch(s->graph, s->ctx->stream), "graph launch");
+    } else {
+      if ((rc = enqueue_step(s, want_lambda, stage_ms ? ev : nullptr))) return rc;
+    }
+    if ((rc = pull_scalars(s))) return rc;
+    if (stage_ms && h.active == 0 && h.status != kFinished) {
+      const int ns = s->time_scheme == FRG_TIME_SSP_RK2 ? 2 : 3;
+      for (int k = 0; k < ns; ++k) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+        acc[k] += ms;
+      }
+      ++nt;
+    }
+    if (h.status != kRunning) break;
+  }
+  if (stage_ms) {
+    for (int k = 0; k < 3; ++k) stage_ms[k] = nt ? acc[k] / (double)nt : 0.0;
+    for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+  }
+  if ((rc = finish_run(s))) return rc;
+  if (out) {
+    out->status = h.status == kFinished ? FRG_OK : h.status;
+    out->n_steps = h.n_steps;
+    out->t = h.t;
+  }
+  return FRG_OK;
+}
+
+int frg_step(frg_solve* s, double dt, int* step_status) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  if (!(dt > 0.0)) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "dt must be > 0");
+  frg_result r;
+  int rc = run_steps(s, INFINITY, 0.0, dt, 1, &r, false);
+  if (rc) return rc;
+  if (step_status) *step_status = r.status == FRG_DIVERGED ? FRG_DIVERGED : FRG_OK;
+  return FRG_OK;
+}
+
+int frg_time_stages(frg_solve* s, int64_t nsteps, double cfl, double fixed_dt, double* stage_ms, frg_result* out) {
+  if (!s || !stage_ms) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  if (nsteps < 1) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "nsteps must be >= 1");
+  return run_steps(s, INFINITY, cfl, fixed_dt, nsteps, out, false, stage_ms);
+}
+
+int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps, frg_result* out) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  if (max_steps < 1) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "max_steps must be >= 1");
+  if (!(fixed_dt > 0.0) && !(cfl > 0.0)) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "cfl must be > 0");
+  return run_steps(s, t_final, cfl, fixed_dt, max_steps, out, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,167 @@
+// Internal structures shared by the host runtime and the sm_100a kernels.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/frforge_cuda.h"
+
+namespace frg {
+
+constexpr double kEps = 2.220446049250313e-16;  // Julia eps(Float64)
+constexpr int kMaxNp = FRG_MAX_NP;
+
+// Boundary condition as seen by the kernels.
+struct BCDev {
+  int kind;
+  int mode;
+  double st[4];
+  double stb[4];
+  double x0, s0, s1, sdiv;
+};
+
+// Reference-element tables, derived on the host from FROperators.
+//   Dt  = D - gL_xi l_L^T - gR_xi l_R^T   (divergence with the g_DG lift folded in)
+//   DtD = Dt * D                           (BR0 volume term acting on u)
+//   DD  = D * D                            (element-local D(Du) dissipation)
+//   lLD = l_L^T D, lRD = l_R^T D           (face traces of D u)
+//   Vinv = V^{-1}                           (modal coefficients of the sensor)
+// Row-major [i][k] so that a thread computing output i reads a contiguous row.
+template <int NP>
+struct OpsT {
+  double Dt[NP][NP];
+  double DtD[NP][NP];
+  double DD[NP][NP];
+  double Vinv[NP][NP];
+  double lL[NP], lR[NP], lLD[NP], lRD[NP], gL[NP], gR[NP];
+  double xi[NP];
+};
+
+// Host copy of all tables for one (p, points) pair (NP <= kMaxNp).
+struct HostOps {
+  int p = 0, np = 0, points = 0;
+  double xi[kMaxNp], w[kMaxNp];
+  double D[kMaxNp][kMaxNp];  // row-major D[i][k]
+  double lL[kMaxNp], lR[kMaxNp], gLxi[kMaxNp], gRxi[kMaxNp], gL[kMaxNp], gR[kMaxNp];
+  double V[kMaxNp][kMaxNp];  // V[j][k] = P_k(xi_j)
+  // derived
+  double Dt[kMaxNp][kMaxNp], DtD[kMaxNp][kMaxNp], DD[kMaxNp][kMaxNp], Vinv[kMaxNp][kMaxNp];
+  double lLD[kMaxNp], lRD[kMaxNp];
+};
+
+// 2D mesh on the device.  Affine meshes keep only per-column / per-row
+// spacing; curved meshes add per-solution-point metric fields and
+// per-face-point normals (the MeshMetrics2D arrays).
+struct Mesh2Dev {
+  int nx, ny, nel;
+  int px, py;  // periodic in x / y
+  const double* xc;  // [nx] column centres (xL+xR)/2
+  const double* Jx;  // [nx] dx/2
+  const double* dx;  // [nx]
+  const double* yc;
+  const double* Jy;
+  const double* dy;
+  const double* hchar;  // [nel]
+  int curved;
+  const double* m_xxi;  // [nel*np2] per SP, element-major
+  const double* m_xeta;
+  const double* m_yxi;
+  const double* m_yeta;
+  const double* m_rJ;     // 1/J
+  const double* f_nx[4];  // [nel*np] per face point; faces W,E,S,N
+  const double* f_ny[4];
+  const double* f_sJ[4];
+  const unsigned char* solid;  // [nel] or null
+  int wavy;
+  double amp;
+  BCDev bc[4];  // left right bottom top
+};
+
+struct Mesh1Dev {
+  int nel;
+  int periodic;
+  const double* xc;  // [nel] element centres
+  const double* J;   // [nel] dx/2
+  const double* dx;  // [nel]
+  BCDev bc[2];
+};
+
+// Per-solve device scalars: time, dt, loop control and status word.
+struct DevScalars {
+  double t;        // time of the state in buffer 0
+  double t0;       // step start time
+  double dt;       // dt of the step in flight
+  double t_final;
+  double cfl;
+  double fixed_dt;  // > 0: fixed step
+  double hmin;      // 2D: min h_char; 1D: min dx
+  unsigned long long lam_bits;  // max wave speed of the current state (non-negative double bits)
+  unsigned int flags;           // bit0: du non-finite, bit1: state non-finite
+  int status;                   // 0 running, FRG_DIVERGED, FRG_MAX_STEPS, 3 finished
+  int active;                   // the step in flight runs
+  int diverged_stage;           // 1..3, 4 = end-of-step state check
+  int two_p1;                   // 2p+1
+  int pad;
+  long long n_steps;
+  long long max_steps;
+  long long residual_evals;
+};
+
+enum : int { kRunning = 0, kFinished = 3 };
+
+// Stage kernel launch parameters (shared by the 1D and 2D kernels).
+struct StageBufs {
+  const double* us;   // stage input state
+  const double* u0;   // step-start state (stages 2, 3)
+  double* uout;       // output state (may alias u0)
+  double* du_out;     // residual-only output
+  const double* eps_in;
+  double* eps_out;
+  double a, b, c;  // u_new = a*u0 + b*us + (c*dt)*du
+  int stage;       // 1..3 (time offset 0, dt, dt/2 for RK3; 0, dt for RK2)
+  int mode;        // kModeStage / kModeResidual / kModePrime / kModeSense
+  int rk2;
+  int want_lambda;  // accumulate the CFL wave speed of the output state
+  int want_eps;     // compute the element viscosity of the output state
+  int use_sc;       // honour DevScalars active/flags (graph execution)
+  DevScalars* sc;
+  double* sigma_out;  // kModeSense
+};
+
+enum : int { kModeStage = 0, kModeResidual = 1, kModePrime = 2, kModeSense = 3 };
+
+struct Phys {
+  double gamma, g1;  // gamma, gamma-1
+  double c_av, kappa, s0, eps_floor;
+  int p, pm;  // p, max(p,1)
+};
+
+enum : int { kAvNone = 0, kAvBR0 = 1, kAvDD = 2 };
+
+// ---- host helpers (frg_host.cpp) ----
+int build_host_ops(int p, int points, HostOps* out);
+int host_ops_from_caller(const frg_operators* in, HostOps* out);
+void derive_tables(HostOps* o);
+void julia_linspace(double a, double b, int len, double* out);
+
+// ---- kernel launchers (frg_launch_np*.cu) ----
+struct Launch2D {
+  const HostOps* ops;
+  Mesh2Dev mesh;
+  Phys phys;
+  int flux;  // FRG_FLUX_*
+  int av;    // kAv*
+};
+struct Launch1D {
+  const HostOps* ops;
+  Mesh1Dev mesh;
+  Phys phys;
+  int flux;
+  int av;
+};
+// Returns 0 or a CUDA error code.
+int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream);
+int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream);
+int stage2d_smem_bytes(int np, int av);
+
+}  // namespace frg

@@ -1,0 +1,2 @@
+#include "frg_launch.cuh"
+FRG_INSTANTIATE_NP(3)

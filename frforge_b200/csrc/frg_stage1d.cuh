@@ -1,0 +1,310 @@
+// Fused 1D FR stage kernel for sm_100a (FP64).
+//
+// Same phase structure as the 2D kernel: a CTA stages TX elements plus one
+// halo element on each side, computes traces and the interface flux of every
+// face once (compute_interface_fluxes!, src/fr/Residual.jl:24-115), the
+// strong-form volume + g_DG lift (Residual.jl:187-208), the BR0 or D(Du)
+// dissipation (src/capturing/PerssonAV.jl:203-351), the SSP-RK stage
+// combination, and for the new state the Persson sensor (PerssonAV.jl:116-135),
+// element viscosity (:158-177) and the CFL wave speed (SSP_RK3.jl:8-24).
+#pragma once
+
+#include "frg_device.cuh"
+
+namespace frg {
+
+template <int NP>
+struct Tile1D {
+  static constexpr int TX = 64;
+};
+
+template <int NP>
+struct Smem1D {
+  static constexpr int NEQ = 3, TX = Tile1D<NP>::TX, NSLOT = TX + 2;
+  static constexpr int oU = 0;
+  static constexpr int oF = oU + NSLOT * NEQ * NP;
+  static constexpr int oG = oF + TX * NEQ * NP;
+  static constexpr int oFace = oG + TX * NEQ * NP;  // [TX+1][8]: fhat[3], ghat[3]
+  static constexpr int oSlot = oFace + (TX + 1) * 8;  // eps, J, dx
+  static constexpr int oRed = oSlot + NSLOT * 3;
+  static constexpr int nDoubles = oRed + 32;
+  static constexpr int nInts = NSLOT * 2;
+  static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
+};
+
+template <int NP, int FLUX, int AV>
+__global__ void __launch_bounds__(256)
+    stage1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const StageBufs B) {
+  using S = Smem1D<NP>;
+  constexpr int NEQ = 3, TX = S::TX, NSLOT = S::NSLOT;
+  constexpr bool kBR0 = (AV == kAvBR0);
+  constexpr bool kAV = (AV != kAvNone);
+  extern __shared__ __align__(16) double smem[];
+  double* sU = smem + S::oU;
+  double* sF = smem + S::oF;
+  double* sG = smem + S::oG;
+  double* sFace = smem + S::oFace;
+  double* sEps = smem + S::oSlot;
+  double* sJ = sEps + NSLOT;
+  double* sDx = sJ + NSLOT;
+  double* sRed = smem + S::oRed;
+  int* sEl = reinterpret_cast<int*>(smem + S::nDoubles);
+  int* sOwn = sEl + NSLOT;
+
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nel = M.nel;
+  const size_t cs = (size_t)nel * NP;
+
+  double dt = 0.0, tstage = 0.0;
+  if (B.use_sc) {
+    if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
+    dt = B.sc->dt;
+    const double t0 = B.sc->t0;
+    tstage = (B.stage == 1) ? t0 : (B.stage == 2 ? t0 + dt : t0 + dt / 2.0);
+  } else if (B.sc) {
+    tstage = B.sc->t;
+    dt = B.sc->dt;
+  }
+  (void)tstage;
+  const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
+  const int x0 = blockIdx.x * TX;
+
+  for (int s = tid; s < NSLOT; s += nthr) {
+    int g = x0 + s - 1, el = -1, own = 0;
+    bool ok = true, wrap = false;
+    if (g < 0) {
+      if (M.periodic) { g += nel; wrap = true; } else ok = false;
+    } else if (g >= nel) {
+      if (g == nel && M.periodic) { g = 0; wrap = true; } else ok = false;
+    }
+    if (ok) {
+      el = g;
+      own = (s >= 1 && s <= TX && !wrap);
+      if (prime && !own) el = -1;
+    }
+    if (el >= 0) {
+      sJ[s] = M.J[el];
+      sDx[s] = M.dx[el];
+      sEps[s] = (kAV && !prime) ? B.eps_in[el] : 0.0;
+    }
+    sEl[s] = el;
+    sOwn[s] = own;
+  }
+  __syncthreads();
+
+  for (int idx = tid; idx < NEQ * NSLOT * NP; idx += nthr) {
+    const int r = idx % (NSLOT * NP), c = idx / (NSLOT * NP);
+    const int s = r / NP, k = r % NP;
+    const int el = sEl[s];
+    if (el >= 0) sU[(s * NEQ + c) * NP + k] = __ldg(&B.us[c * cs + (size_t)el * NP + k]);
+  }
+  __syncthreads();
+
+  if (!prime) {
+    // P1: physical flux at own solution points
+    for (int idx = tid; idx < TX * NP; idx += nthr) {
+      const int k = idx % NP, o = idx / NP, s = o + 1;
+      if (!sOwn[s]) continue;
+      double U[3], F[3];
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) U[c] = sU[(s * NEQ + c) * NP + k];
+      flux1(P.g1, U, F);
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) sF[(o * NEQ + c) * NP + k] = F[c];
+    }
+    // P2: faces f = 0..TX between slots f and f+1
+    for (int f = tid; f < TX + 1; f += nthr) {
+      const int sA = f, sB = f + 1;
+      double* out = sFace + f * 8;
+      if (!(sOwn[sA] || sOwn[sB])) continue;
+      const int eA = sEl[sA], eB = sEl[sB];
+      double uA[3], uB[3], gA[3], gB[3];
+      if (eA >= 0) {
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          double su = 0.0, sg = 0.0;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double v = sU[(sA * NEQ + c) * NP + i];
+            su += ops.lR[i] * v;
+            if (kBR0) sg += ops.lRD[i] * v;
+          }
+          uA[c] = su;
+          gA[c] = sg;
+        }
+      }
+      if (eB >= 0) {
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          double su = 0.0, sg = 0.0;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double v = sU[(sB * NEQ + c) * NP + i];
+            su += ops.lL[i] * v;
+            if (kBR0) sg += ops.lLD[i] * v;
+          }
+          uB[c] = su;
+          gB[c] = sg;
+        }
+      }
+      double fh[3], gh[3] = {0.0, 0.0, 0.0};
+      if (eA >= 0 && eB >= 0) {
+        iflux1<FLUX>(P.gamma, P.g1, uA, uB, fh);
+        if (kBR0) {
+          const double sa = sEps[sA] / sJ[sA], sb = sEps[sB] / sJ[sB];
+          const double tau = br0_tau(sEps[sA], sEps[sB], sDx[sA], sDx[sB], P.p);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = 0.5 * (sa * gA[c] + sb * gB[c]) - tau * (uB[c] - uA[c]);
+        }
+      } else if (eB >= 0) {  // domain left end (Residual.jl:63-89)
+        double ug[3];
+        exterior1(M.bc[0], uB, -1.0, ug);
+        iflux1<FLUX>(P.gamma, P.g1, ug, uB, fh);
+        if (kBR0) {
+          const double sb = sEps[sB] / sJ[sB];
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = sb * gB[c];
+        }
+      } else {  // domain right end (Residual.jl:91-112)
+        double ug[3];
+        exterior1(M.bc[1], uA, 1.0, ug);
+        iflux1<FLUX>(P.gamma, P.g1, uA, ug, fh);
+        if (kBR0) {
+          const double sa = sEps[sA] / sJ[sA];
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = sa * gA[c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) {
+        out[c] = fh[c];
+        out[4 + c] = gh[c];
+      }
+    }
+    __syncthreads();
+    // P3: volume + lift (+ dissipation) per (element, component)
+    for (int idx = tid; idx < TX * NEQ; idx += nthr) {
+      const int c = idx % NEQ, o = idx / NEQ, s = o + 1;
+      if (!sOwn[s]) continue;
+      double Fl[NP], Ul[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        Fl[k] = sF[(o * NEQ + c) * NP + k];
+        Ul[k] = sU[(s * NEQ + c) * NP + k];
+      }
+      const double fL = sFace[o * 8 + c], fR = sFace[(o + 1) * 8 + c];
+      const double gLh = kBR0 ? sFace[o * 8 + 4 + c] : 0.0;
+      const double gRh = kBR0 ? sFace[(o + 1) * 8 + 4 + c] : 0.0;
+      const double J = sJ[s], rJ = 1.0 / J;
+      const double ev = kAV ? sEps[s] / (J * J) : 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        double acc = ops.gL[j] * fL + ops.gR[j] * fR;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Fl[k];
+        double r = -acc * rJ;
+        if (kBR0) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DtD[j][m] * Ul[m];
+          r += ev * av + (ops.gL[j] * gLh + ops.gR[j] * gRh) * rJ;
+        } else if (AV == kAvDD) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DD[j][m] * Ul[m];
+          r += ev * av;
+        }
+        sG[(o * NEQ + c) * NP + j] = r;
+      }
+    }
+    __syncthreads();
+    // P5: stage combination
+    int bad_du = 0, bad_u = 0;
+    const double cdt = B.c * dt;
+    for (int idx = tid; idx < NEQ * TX * NP; idx += nthr) {
+      const int r = idx % (TX * NP), c = idx / (TX * NP);
+      const int o = r / NP, k = r % NP, s = o + 1;
+      if (!sOwn[s]) continue;
+      const double du = sG[(o * NEQ + c) * NP + k];
+      const size_t gi = c * cs + (size_t)sEl[s] * NP + k;
+      if (B.mode == kModeResidual) {
+        B.du_out[gi] = du;
+        bad_du |= !isfinite(du);
+        continue;
+      }
+      const double us = sU[(s * NEQ + c) * NP + k];
+      const double u0 = (B.stage == 1) ? us : B.u0[gi];
+      const double un = (B.a * u0 + B.b * us) + cdt * du;
+      B.uout[gi] = un;
+      sF[(o * NEQ + c) * NP + k] = un;
+      bad_du |= !isfinite(du);
+      bad_u |= !isfinite(un);
+    }
+    const int any_du = __syncthreads_or(bad_du);
+    const int any_u = __syncthreads_or(bad_u);
+    if (tid == 0 && (any_du || any_u) && B.sc)
+      atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
+    if (B.mode == kModeResidual) return;
+  } else {
+    for (int idx = tid; idx < TX * NEQ * NP; idx += nthr) {
+      const int o = idx / (NEQ * NP), s = o + 1;
+      if (sOwn[s]) sF[idx] = sU[(s * NEQ) * NP + (idx - o * NEQ * NP)];
+    }
+    __syncthreads();
+  }
+
+  // P6: sensor, eps and CFL wave speed of the new state
+  if (!(kAV || B.want_lambda || B.mode == kModeSense)) return;
+  double lmax = 0.0;
+  double* sWS = sG;
+  for (int idx = tid; idx < TX * NP; idx += nthr) {
+    const int k = idx % NP, o = idx / NP, s = o + 1;
+    if (!sOwn[s]) continue;
+    double U[3];
+#pragma unroll
+    for (int c = 0; c < NEQ; ++c) U[c] = sF[(o * NEQ + c) * NP + k];
+    const double w = wave_speed1(P.gamma, P.g1, U);
+    sWS[o * NP + k] = w;
+    lmax = jmax(lmax, w);
+  }
+  if (B.want_lambda) {
+    for (int off = 16; off > 0; off >>= 1) lmax = jmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+    if ((tid & 31) == 0) sRed[tid >> 5] = lmax;
+  }
+  __syncthreads();
+  if (B.want_lambda && tid < 32) {
+    double v = (tid < (nthr >> 5)) ? sRed[tid] : 0.0;
+    for (int off = 16; off > 0; off >>= 1) v = jmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if (tid == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, v);
+  }
+  if (!(kAV || B.mode == kModeSense)) return;
+  for (int o = tid; o < TX; o += nthr) {
+    const int s = o + 1;
+    if (!sOwn[s]) continue;
+    const int el = sEl[s];
+    double rho[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) rho[k] = sF[(o * NEQ) * NP + k];
+    double etot = 0.0, ehigh = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      double a = 0.0;
+#pragma unroll
+      for (int k = 0; k < NP; ++k) a += ops.Vinv[i][k] * rho[k];
+      etot += a * a;
+      if (i == NP - 1) ehigh = a * a;
+    }
+    const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
+    if (B.mode == kModeSense) {
+      B.sigma_out[el] = sig;
+      continue;
+    }
+    double lam = 0.0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) lam = jmax(lam, sWS[o * NP + k]);
+    lam = jmax(lam, kEps);
+    B.eps_out[el] = (sig > 0.0) ? P.c_av * sig * (sDx[s] / (double)P.pm) * lam : 0.0;
+  }
+}
+
+}  // namespace frg

@@ -1,0 +1,625 @@
+// Fused 2D FR stage kernel for sm_100a (FP64).
+//
+// One CTA owns a TX x TY tile of elements and stages the tile plus a
+// one-element halo ring (no corners) of the stage input in shared memory.
+// Everything a stage needs happens on chip:
+//   P0  load u (tile + halo) and the element viscosities eps (tile + halo)
+//   P1  physical fluxes -> contravariant F~, G~ at every own solution point
+//       (Residual2D.jl:342-352)
+//   P2  every face point of the tile once: u traces of both sides
+//       (face_trace!, Residual2D.jl:9-48), Rusanov/HLLC or the boundary
+//       ghost flux times sJ (Residual2D.jl:173-334), and for BR0 the g traces
+//       and the averaged viscous flux g^ (PerssonAV2D.jl:228-350)
+//   P3  xi-direction divergence + g_DG lift (Residual2D.jl:354-374) and the
+//       BR0 / D(Du) x-terms (PerssonAV2D.jl:135-194, :352-375)
+//   P4  eta-direction terms (Residual2D.jl:376-396, PerssonAV2D.jl:376-395)
+//   P5  SSP-RK stage combination (SSP_RK3.jl:135-164) written straight to
+//       HBM -- du never leaves the chip -- plus non-finite flags
+//   P6  sensor of the NEW state (sense!, PerssonAV2D.jl:20-59), element
+//       viscosity eps for the next stage (element_viscosities_2d,
+//       PerssonAV2D.jl:89-109) and the CFL wave speed (compute_dt,
+//       SSP_RK3.jl:126-133) as one atomic max per CTA.
+// Halo values come from the neighbouring tiles' own loads, so they are
+// L2 hits; DRAM traffic per stage is the algorithmic u_s + u0 + u_out.
+#pragma once
+
+#include "frg_device.cuh"
+
+namespace frg {
+
+template <int NP>
+struct Tile2D;
+// Tile shapes (elements).  Chosen so a CTA's shared memory lets 2 CTAs
+// reside per SM for P <= 4.
+template <>
+struct Tile2D<2> {
+  static constexpr int TX = 16, TY = 8;
+};
+template <>
+struct Tile2D<3> {
+  static constexpr int TX = 8, TY = 8;
+};
+template <>
+struct Tile2D<4> {
+  static constexpr int TX = 8, TY = 4;
+};
+template <>
+struct Tile2D<5> {
+  static constexpr int TX = 4, TY = 4;
+};
+template <>
+struct Tile2D<6> {
+  static constexpr int TX = 4, TY = 4;
+};
+
+template <int NP, int TX, int TY>
+struct Smem2D {
+  static constexpr int NEQ = 4, NP2 = NP * NP;
+  static constexpr int BX = TX + 2, BY = TY + 2, NSLOT = BX * BY, NOWN = TX * TY;
+  static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
+  // doubles
+  static constexpr int oU = 0;
+  static constexpr int oF = oU + NSLOT * NEQ * NP2;
+  static constexpr int oG = oF + NOWN * NEQ * NP2;
+  static constexpr int oFV = oG + NOWN * NEQ * NP2;
+  static constexpr int oFH = oFV + NFV * NP * 8;
+  static constexpr int oSlot = oFH + NFH * NP * 8;  // per slot: eps, Jx, Jy, dx, dy
+  static constexpr int oRed = oSlot + NSLOT * 5;    // reduction scratch
+  static constexpr int nDoubles = oRed + 32;
+  // ints after the doubles: element id, flags
+  static constexpr int nInts = NSLOT * 2 + 8;
+  static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
+};
+
+constexpr int kStageThreads = 256;
+
+// slot flag bits
+enum : int { kSlotOwn = 1, kSlotWrap = 2, kSlotSolid = 4 };
+
+template <int NP, int FLUX, int AV>
+__global__ void __launch_bounds__(kStageThreads, 2)
+    stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
+  constexpr int TX = Tile2D<NP>::TX, TY = Tile2D<NP>::TY;
+  using S = Smem2D<NP, TX, TY>;
+  constexpr int NEQ = 4, NP2 = NP * NP;
+  constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, NOWN = S::NOWN;
+  constexpr int NFV = S::NFV, NFH = S::NFH;
+  constexpr bool kBR0 = (AV == kAvBR0);
+  constexpr bool kAV = (AV != kAvNone);
+
+  extern __shared__ __align__(16) double smem[];
+  double* sU = smem + S::oU;
+  double* sF = smem + S::oF;
+  double* sG = smem + S::oG;
+  double* sFV = smem + S::oFV;
+  double* sFH = smem + S::oFH;
+  double* sEps = smem + S::oSlot;
+  double* sJx = sEps + NSLOT;
+  double* sJy = sJx + NSLOT;
+  double* sDx = sJy + NSLOT;
+  double* sDy = sDx + NSLOT;
+  double* sRed = smem + S::oRed;
+  int* sEl = reinterpret_cast<int*>(smem + S::nDoubles);
+  int* sFlag = sEl + NSLOT;
+  int* sMisc = sFlag + NSLOT;
+
+  const int tid = threadIdx.x;
+  const int nthr = blockDim.x;
+  const int nx = M.nx, ny = M.ny;
+  const size_t cs = (size_t)M.nel * NP2;  // component stride
+
+  // graph execution: skip finished / diverged solves
+  double dt = 0.0, tstage = 0.0;
+  if (B.use_sc) {
+    if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
+    dt = B.sc->dt;
+    const double t0 = B.sc->t0;
+    tstage = (B.stage == 1) ? t0 : (B.stage == 2 ? t0 + dt : t0 + dt / 2.0);
+  } else if (B.sc) {
+    tstage = B.sc->t;
+    dt = B.sc->dt;
+  }
+  const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
+
+  const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
+
+  // ---------------------------------------------------------------- slots
+  for (int s = tid; s < NSLOT; s += nthr) {
+    const int bx = s % BX, by = s / BX;
+    const bool corner = (bx == 0 || bx == BX - 1) && (by == 0 || by == BY - 1);
+    int gx = tx0 + bx - 1, gy = ty0 + by - 1;
+    int el = -1, fl = 0;
+    if (!corner) {
+      const bool ownpos = (bx >= 1 && bx <= TX && by >= 1 && by <= TY);
+      bool ok = true, wrap = false;
+      if (gx < 0) {
+        if (M.px) { gx += nx; wrap = true; } else ok = false;
+      } else if (gx >= nx) {
+        if (gx == nx && M.px) { gx = 0; wrap = true; } else ok = false;
+      }
+      if (gy < 0) {
+        if (M.py) { gy += ny; wrap = true; } else ok = false;
+      } else if (gy >= ny) {
+        if (gy == ny && M.py) { gy = 0; wrap = true; } else ok = false;
+      }
+      if (ok) {
+        el = gy * nx + gx;
+        if (ownpos && !wrap) fl |= kSlotOwn;
+        if (wrap) fl |= kSlotWrap;
+        if (M.solid && M.solid[el]) fl |= kSlotSolid;
+        if (prime && !(fl & kSlotOwn)) el = -1;  // prime/sense: own elements only
+      }
+      if (el >= 0) {
+        sJx[s] = M.Jx[gx];
+        sJy[s] = M.Jy[gy];
+        sDx[s] = M.dx[gx];
+        sDy[s] = M.dy[gy];
+        sEps[s] = (kAV && !prime) ? B.eps_in[el] : 0.0;
+      }
+    }
+    sEl[s] = el;
+    sFlag[s] = fl;
+  }
+  if (tid == 0) sMisc[0] = 0;
+  __syncthreads();
+
+  // ------------------------------------------------------------- P0 load
+  {
+    constexpr int ROW = BX * NP2;
+    const double* src = B.us;
+    for (int idx = tid; idx < BY * NEQ * ROW; idx += nthr) {
+      const int r = idx % ROW;
+      const int t = idx / ROW;
+      const int c = t % NEQ, by = t / NEQ;
+      const int bx = r / NP2, k = r % NP2;
+      const int s = by * BX + bx;
+      const int el = sEl[s];
+      if (el >= 0) sU[(s * NEQ + c) * NP2 + k] = __ldg(&src[c * cs + (size_t)el * NP2 + k]);
+    }
+  }
+  __syncthreads();
+
+  if (!prime) {
+    // ------------------------------------------------------- P1 fluxes
+    for (int idx = tid; idx < NOWN * NP2; idx += nthr) {
+      const int k = idx % NP2, o = idx / NP2;
+      const int s = (o / TX + 1) * BX + (o % TX) + 1;
+      if (!(sFlag[s] & kSlotOwn) || (sFlag[s] & kSlotSolid)) continue;
+      double U[4], F[4], G[4];
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) U[c] = sU[(s * NEQ + c) * NP2 + k];
+      flux_xy(P.g1, U, F, G);
+      if (M.curved) {
+        const size_t m = (size_t)sEl[s] * NP2 + k;
+        const double xxi = M.m_xxi[m], xeta = M.m_xeta[m], yxi = M.m_yxi[m], yeta = M.m_yeta[m];
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          sF[(o * NEQ + c) * NP2 + k] = yeta * F[c] - xeta * G[c];
+          sG[(o * NEQ + c) * NP2 + k] = -yxi * F[c] + xxi * G[c];
+        }
+      } else {
+        const double jy = sJy[s], jx = sJx[s];
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          sF[(o * NEQ + c) * NP2 + k] = jy * F[c];
+          sG[(o * NEQ + c) * NP2 + k] = jx * G[c];
+        }
+      }
+    }
+
+    // ------------------------------------------------------- P2 faces
+    for (int idx = tid; idx < (NFV + NFH) * NP; idx += nthr) {
+      const bool vert = idx < NFV * NP;
+      const int id2 = vert ? idx : idx - NFV * NP;
+      const int q = id2 % NP, f = id2 / NP;
+      int sA, sB;
+      if (vert) {
+        const int fx = f % (TX + 1), fy = f / (TX + 1);
+        sA = (fy + 1) * BX + fx;
+        sB = sA + 1;
+      } else {
+        const int fx = f % TX, fy = f / TX;
+        sA = fy * BX + fx + 1;
+        sB = sA + BX;
+      }
+      const int flA = sFlag[sA], flB = sFlag[sB];
+      double* out = (vert ? sFV : sFH) + (f * NP + q) * 8;
+      if (!((flA | flB) & kSlotOwn)) continue;
+      const int eA = sEl[sA], eB = sEl[sB];
+      double uA[4], uB[4], gA[4], gB[4];
+      // traces: A's east/north face, B's west/south face
+      if (eA >= 0) {
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          const double* a = sU + (sA * NEQ + c) * NP2;
+          double su = 0.0, sg = 0.0;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double v = vert ? a[i + NP * q] : a[q + NP * i];
+            su += ops.lR[i] * v;
+            if (kBR0) sg += ops.lRD[i] * v;
+          }
+          uA[c] = su;
+          gA[c] = sg;
+        }
+      }
+      if (eB >= 0) {
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          const double* b = sU + (sB * NEQ + c) * NP2;
+          double su = 0.0, sg = 0.0;
+#pragma unroll
+          for (int i = 0; i < NP; ++i) {
+            const double v = vert ? b[i + NP * q] : b[q + NP * i];
+            su += ops.lL[i] * v;
+            if (kBR0) sg += ops.lLD[i] * v;
+          }
+          uB[c] = su;
+          gB[c] = sg;
+        }
+      }
+      double fh[4] = {0.0, 0.0, 0.0, 0.0};
+      double gh[4] = {0.0, 0.0, 0.0, 0.0};
+      const int fE = vert ? 1 : 3, fW = vert ? 0 : 2;  // face slots E/N and W/S
+      if (eA >= 0 && eB >= 0) {
+        const bool solA = flA & kSlotSolid, solB = flB & kSlotSolid;
+        const bool wrapf = (flA | flB) & kSlotWrap;
+        if (wrapf && (solA || solB)) {
+          // the reference never writes these slots (Residual2D.jl:220, :302)
+        } else if (solA && solB) {
+        } else if (solA || solB) {
+          // wall between a solid and a fluid element (Residual2D.jl:186-200)
+          const bool fluidB = solA;
+          const int e = fluidB ? eB : eA;
+          const int face = fluidB ? fW : fE;
+          double nxo, nyo, sJ;
+          if (M.curved) {
+            nxo = M.f_nx[face][(size_t)e * NP + q];
+            nyo = M.f_ny[face][(size_t)e * NP + q];
+            sJ = M.f_sJ[face][(size_t)e * NP + q];
+          } else {
+            nxo = vert ? (fluidB ? -1.0 : 1.0) : 0.0;
+            nyo = vert ? 0.0 : (fluidB ? -1.0 : 1.0);
+            sJ = vert ? sJy[fluidB ? sB : sA] : sJx[fluidB ? sB : sA];
+          }
+          const double* ui = fluidB ? uB : uA;
+          double ug[4];
+          reflect2(ui, nxo, nyo, ug);
+          if (fluidB)
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh);
+          else
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
+        } else {
+          double nnx, nny, sJ;
+          if (M.curved) {
+            nnx = M.f_nx[fE][(size_t)eA * NP + q];
+            nny = M.f_ny[fE][(size_t)eA * NP + q];
+            sJ = M.f_sJ[fE][(size_t)eA * NP + q];
+          } else {
+            nnx = vert ? 1.0 : 0.0;
+            nny = vert ? 0.0 : 1.0;
+            sJ = vert ? sJy[sA] : sJx[sA];
+          }
+          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
+        }
+        if (kBR0) {
+          const double JA = vert ? sJx[sA] : sJy[sA], JB = vert ? sJx[sB] : sJy[sB];
+          const double sa = sEps[sA] / JA, sb = sEps[sB] / JB;
+          const double tau =
+              br0_tau(sEps[sA], sEps[sB], vert ? sDx[sA] : sDy[sA], vert ? sDx[sB] : sDy[sB], P.p);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c)
+            gh[c] = 0.5 * (sa * gA[c] + sb * gB[c]) - tau * (uB[c] - uA[c]);
+        }
+      } else {
+        // domain boundary: A missing (left/bottom) or B missing (right/top)
+        const bool haveB = eB >= 0;
+        const int s = haveB ? sB : sA;
+        const int e = haveB ? eB : eA;
+        const int fl = haveB ? flB : flA;
+        const int face = haveB ? fW : fE;
+        const BCDev& bc = M.bc[vert ? (haveB ? 0 : 1) : (haveB ? 2 : 3)];
+        const double* ui = haveB ? uB : uA;
+        if (!(fl & kSlotSolid)) {
+          double nxo, nyo, sJ;
+          if (M.curved) {
+            nxo = M.f_nx[face][(size_t)e * NP + q];
+            nyo = M.f_ny[face][(size_t)e * NP + q];
+            sJ = M.f_sJ[face][(size_t)e * NP + q];
+          } else {
+            nxo = vert ? (haveB ? -1.0 : 1.0) : 0.0;
+            nyo = vert ? 0.0 : (haveB ? -1.0 : 1.0);
+            sJ = vert ? sJy[s] : sJx[s];
+          }
+          // face point coordinates (physical_xy, MeshMetrics2D.jl:49-74)
+          const int gx = e % nx, gy = e / nx;
+          double X, Y;
+          if (vert) {
+            X = M.xc[gx] + M.Jx[gx] * (haveB ? -1.0 : 1.0);
+            Y = M.yc[gy] + M.Jy[gy] * ops.xi[q];
+          } else {
+            X = M.xc[gx] + M.Jx[gx] * ops.xi[q];
+            Y = M.yc[gy] + M.Jy[gy] * (haveB ? -1.0 : 1.0);
+          }
+          if (M.wavy) X = X + M.amp * sin(6.283185307179586 * Y) * sin(3.141592653589793 * X);
+          double ug[4];
+          exterior<4>(bc, ui, nxo, nyo, X, tstage, ug);
+          if (haveB)
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh);
+          else
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
+        }
+        if (kBR0) {
+          const double Jd = vert ? sJx[s] : sJy[s];
+          const double sc = sEps[s] / Jd;
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = sc * (haveB ? gB[c] : gA[c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) {
+        out[c] = fh[c];
+        out[4 + c] = gh[c];
+      }
+    }
+    __syncthreads();
+
+    // ------------------------------------------------ P3 xi-direction
+    for (int idx = tid; idx < NOWN * NP * NEQ; idx += nthr) {
+      const int c = idx % NEQ;
+      const int t = idx / NEQ;
+      const int j = t % NP, o = t / NP;
+      const int ox = o % TX, oy = o / TX;
+      const int s = (oy + 1) * BX + ox + 1;
+      if (!(sFlag[s] & kSlotOwn)) continue;
+      double* Fo = sF + (o * NEQ + c) * NP2;
+      if (sFlag[s] & kSlotSolid) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) Fo[i + NP * j] = 0.0;
+        continue;
+      }
+      const double* Uo = sU + (s * NEQ + c) * NP2;
+      double Fl[NP], Ul[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        Fl[k] = Fo[k + NP * j];
+        Ul[k] = Uo[k + NP * j];
+      }
+      const int fW = oy * (TX + 1) + ox;
+      const double fhW = sFV[(fW * NP + j) * 8 + c];
+      const double fhE = sFV[((fW + 1) * NP + j) * 8 + c];
+      const double ghW = kBR0 ? sFV[(fW * NP + j) * 8 + 4 + c] : 0.0;
+      const double ghE = kBR0 ? sFV[((fW + 1) * NP + j) * 8 + 4 + c] : 0.0;
+      const double jx = sJx[s];
+      const double rJa = M.curved ? 0.0 : 1.0 / (jx * sJy[s]);
+      const double ev = kAV ? sEps[s] / (jx * jx) : 0.0;
+      const double rjx = kBR0 ? 1.0 / jx : 0.0;
+      const size_t mrow = (size_t)sEl[s] * NP2 + NP * j;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        double acc = ops.gL[i] * fhW + ops.gR[i] * fhE;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += ops.Dt[i][k] * Fl[k];
+        const double rJ = M.curved ? M.m_rJ[mrow + i] : rJa;
+        double r = -acc * rJ;
+        if (kBR0) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DtD[i][m] * Ul[m];
+          r += ev * av + (ops.gL[i] * ghW + ops.gR[i] * ghE) * rjx;
+        } else if (AV == kAvDD) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DD[i][m] * Ul[m];
+          r += ev * av;
+        }
+        Fo[i + NP * j] = r;
+      }
+    }
+    __syncthreads();
+
+    // ----------------------------------------------- P4 eta-direction
+    for (int idx = tid; idx < NOWN * NP * NEQ; idx += nthr) {
+      const int c = idx % NEQ;
+      const int t = idx / NEQ;
+      const int i = t % NP, o = t / NP;
+      const int ox = o % TX, oy = o / TX;
+      const int s = (oy + 1) * BX + ox + 1;
+      if (!(sFlag[s] & kSlotOwn)) continue;
+      double* Go = sG + (o * NEQ + c) * NP2;
+      const double* Fo = sF + (o * NEQ + c) * NP2;
+      if (sFlag[s] & kSlotSolid) {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) Go[i + NP * j] = 0.0;
+        continue;
+      }
+      const double* Uo = sU + (s * NEQ + c) * NP2;
+      double Gl[NP], Ul[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) {
+        Gl[k] = Go[i + NP * k];
+        Ul[k] = Uo[i + NP * k];
+      }
+      const int fS = oy * TX + ox;
+      const double fhS = sFH[(fS * NP + i) * 8 + c];
+      const double fhN = sFH[((fS + TX) * NP + i) * 8 + c];
+      const double ghS = kBR0 ? sFH[(fS * NP + i) * 8 + 4 + c] : 0.0;
+      const double ghN = kBR0 ? sFH[((fS + TX) * NP + i) * 8 + 4 + c] : 0.0;
+      const double jy = sJy[s];
+      const double rJa = M.curved ? 0.0 : 1.0 / (sJx[s] * jy);
+      const double ev = kAV ? sEps[s] / (jy * jy) : 0.0;
+      const double rjy = kBR0 ? 1.0 / jy : 0.0;
+      const size_t mbase = (size_t)sEl[s] * NP2 + i;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        double acc = ops.gL[j] * fhS + ops.gR[j] * fhN;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Gl[k];
+        const double rJ = M.curved ? M.m_rJ[mbase + NP * j] : rJa;
+        double r = Fo[i + NP * j] - acc * rJ;
+        if (kBR0) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DtD[j][m] * Ul[m];
+          r += ev * av + (ops.gL[j] * ghS + ops.gR[j] * ghN) * rjy;
+        } else if (AV == kAvDD) {
+          double av = 0.0;
+#pragma unroll
+          for (int m = 0; m < NP; ++m) av += ops.DD[j][m] * Ul[m];
+          r += ev * av;
+        }
+        Go[i + NP * j] = r;
+      }
+    }
+    __syncthreads();
+
+    // --------------------------------------------------- P5 epilogue
+    {
+      constexpr int ROW = TX * NP2;
+      int bad_du = 0, bad_u = 0;
+      const double cdt = B.c * dt;
+      for (int idx = tid; idx < TY * NEQ * ROW; idx += nthr) {
+        const int r = idx % ROW;
+        const int t = idx / ROW;
+        const int c = t % NEQ, oy = t / NEQ;
+        const int ox = r / NP2, k = r % NP2;
+        const int o = oy * TX + ox;
+        const int s = (oy + 1) * BX + ox + 1;
+        if (!(sFlag[s] & kSlotOwn)) continue;
+        const double du = sG[(o * NEQ + c) * NP2 + k];
+        const size_t gi = c * cs + (size_t)sEl[s] * NP2 + k;
+        if (B.mode == kModeResidual) {
+          B.du_out[gi] = du;
+          bad_du |= !isfinite(du);
+          continue;
+        }
+        const double us = sU[(s * NEQ + c) * NP2 + k];
+        const double u0 = (B.stage == 1) ? us : B.u0[gi];
+        const double un = (B.a * u0 + B.b * us) + cdt * du;
+        B.uout[gi] = un;
+        sF[(o * NEQ + c) * NP2 + k] = un;
+        bad_du |= !isfinite(du);
+        bad_u |= !isfinite(un);
+      }
+      const int any_du = __syncthreads_or(bad_du);
+      const int any_u = __syncthreads_or(bad_u);
+      if (tid == 0 && (any_du || any_u)) {
+        if (B.sc) atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
+      }
+    }
+    if (B.mode == kModeResidual) return;
+  } else {
+    // prime / sense: the "new" state is the loaded state
+    for (int idx = tid; idx < NOWN * NEQ * NP2; idx += nthr) {
+      const int k = idx % NP2;
+      const int t = idx / NP2;
+      const int c = t % NEQ, o = t / NEQ;
+      const int s = (o / TX + 1) * BX + (o % TX) + 1;
+      if (sFlag[s] & kSlotOwn) sF[(o * NEQ + c) * NP2 + k] = sU[(s * NEQ + c) * NP2 + k];
+    }
+    __syncthreads();
+  }
+
+  // ------------------------------------------ P6 sensor / eps / lambda
+  if (!(kAV || B.want_lambda || B.mode == kModeSense)) return;
+  {
+    double* sWS = sG;             // [NOWN][NP2] wave speeds
+    double* sX = sG + NOWN * NP2;  // [NOWN][NP2] V^{-1} rho
+    double* sPart = sX + NOWN * NP2;  // [NOWN][NP][2]
+    double lmax = 0.0;
+    for (int idx = tid; idx < NOWN * NP2; idx += nthr) {
+      const int k = idx % NP2, o = idx / NP2;
+      const int s = (o / TX + 1) * BX + (o % TX) + 1;
+      if (!(sFlag[s] & kSlotOwn)) continue;
+      double U[4];
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) U[c] = sF[(o * NEQ + c) * NP2 + k];
+      const double w = wave_speed2(P.gamma, P.g1, U);
+      sWS[o * NP2 + k] = w;
+      lmax = jmax(lmax, w);
+    }
+    if (kAV || B.mode == kModeSense) {
+      // X = V^{-1} rho, column by column
+      for (int idx = tid; idx < NOWN * NP; idx += nthr) {
+        const int j = idx % NP, o = idx / NP;
+        const int s = (o / TX + 1) * BX + (o % TX) + 1;
+        if (!(sFlag[s] & kSlotOwn)) continue;
+        const double* rho = sF + (o * NEQ) * NP2;
+        double col[NP];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) col[k] = rho[k + NP * j];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          double a = 0.0;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) a += ops.Vinv[i][k] * col[k];
+          sX[o * NP2 + i + NP * j] = a;
+        }
+      }
+    }
+    if (B.want_lambda) {
+      // block max of the CFL wave speed (compute_dt), one atomic per CTA
+      for (int off = 16; off > 0; off >>= 1) lmax = jmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+      if ((tid & 31) == 0) sRed[tid >> 5] = lmax;
+    }
+    __syncthreads();
+    if (B.want_lambda && tid < 32) {
+      double v = (tid < (nthr >> 5)) ? sRed[tid] : 0.0;
+      for (int off = 16; off > 0; off >>= 1) v = jmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+      if (tid == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, v);
+    }
+    if (!(kAV || B.mode == kModeSense)) return;
+    // Uhat = X V^{-T}: row i energies
+    for (int idx = tid; idx < NOWN * NP; idx += nthr) {
+      const int i = idx % NP, o = idx / NP;
+      const int s = (o / TX + 1) * BX + (o % TX) + 1;
+      if (!(sFlag[s] & kSlotOwn)) continue;
+      double row[NP];
+#pragma unroll
+      for (int k = 0; k < NP; ++k) row[k] = sX[o * NP2 + i + NP * k];
+      double etot = 0.0, ehigh = 0.0;
+#pragma unroll
+      for (int j = 0; j < NP; ++j) {
+        double a = 0.0;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) a += row[k] * ops.Vinv[j][k];
+        const double a2 = a * a;
+        etot += a2;
+        if (i == NP - 1 || j == NP - 1) ehigh += a2;
+      }
+      sPart[(o * NP + i) * 2 + 0] = etot;
+      sPart[(o * NP + i) * 2 + 1] = ehigh;
+    }
+    __syncthreads();
+    for (int o = tid; o < NOWN; o += nthr) {
+      const int s = (o / TX + 1) * BX + (o % TX) + 1;
+      if (!(sFlag[s] & kSlotOwn)) continue;
+      const int el = sEl[s];
+      double etot = 0.0, ehigh = 0.0, lam = 0.0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        etot += sPart[(o * NP + i) * 2 + 0];
+        ehigh += sPart[(o * NP + i) * 2 + 1];
+      }
+#pragma unroll
+      for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * NP2 + k]);
+      lam = jmax(lam, kEps);
+      const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
+      if (B.mode == kModeSense) {
+        B.sigma_out[el] = (sFlag[s] & kSlotSolid) ? 0.0 : sig;
+        continue;
+      }
+      double ev = 0.0;
+      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (M.hchar[el] / (double)P.pm) * lam;
+      B.eps_out[el] = ev;
+    }
+  }
+}
+
+}  // namespace frg

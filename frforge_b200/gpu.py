@@ -1,0 +1,301 @@
+"""GPU execution of the FR residual + SSP-RK path through the C ABI.
+
+These functions are the drop-in counterparts of the reference's
+``residual!`` (src/fr/Residual.jl:161, Residual2D.jl:131), ``sense!``,
+``compute_dt`` (src/time/SSP_RK3.jl:8, :126), ``ssp_rk3_step!`` /
+``ssp_rk2_step!``, ``ssp_rk3!`` / ``ssp_rk2!`` and ``integrate!``
+(src/time/Integrate.jl:9).  Python has no ``!``; a trailing underscore marks
+the in-place functions (``residual_``, ``integrate_``).  The host numpy state
+stays the source of truth between calls: each call uploads ``state.u``,
+runs on the device and writes the result back, like the Julia arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from .methods import AbstractCapturingMethod, NullCapturing
+from .mesh import AbstractBC
+
+_ctx_lock = threading.Lock()
+_contexts = {}
+
+
+class Context:
+    """One frg_ctx (device + CUDA stream); one per host thread and device."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        L.check(L.load().frg_ctx_create(device, C.byref(h)), what=f"frg_ctx_create(device={device})")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            L.load().frg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (wrap with torch.cuda.ExternalStream)."""
+        st = C.c_void_p()
+        L.check(L.load().frg_ctx_get_stream(self.handle, C.byref(st)), what="frg_ctx_get_stream")
+        return st.value or 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def default_context(device: int = 0) -> Context:
+    key = (threading.get_ident(), device)
+    with _ctx_lock:
+        if key not in _contexts:
+            _contexts[key] = Context(device)
+        return _contexts[key]
+
+
+def _bc_struct(bc: AbstractBC) -> L.frg_bc:
+    b = L.frg_bc()
+    b.kind = L.BC_KIND[bc.kind]
+    b.sdiv = 1.0
+    if bc.kind == "dirichlet":
+        st = np.asarray(bc.state, dtype=np.float64).ravel()
+        for i, v in enumerate(st):
+            b.state[i] = v
+    elif bc.kind == "xsplit":
+        for i, v in enumerate(bc.state):
+            b.state[i] = v
+        if bc.state_b is not None:
+            for i, v in enumerate(bc.state_b):
+                b.state_b[i] = v
+        b.mode = 0 if bc.right_reflect else 1
+        b.x0, b.s0, b.s1, b.sdiv = bc.x0, bc.s0, bc.s1, bc.sdiv
+    return b
+
+
+class GpuSolve:
+    """A device-resident solve (frg_solve): descriptor, state buffers, graphs."""
+
+    def __init__(self, state, eq, method: Optional[AbstractCapturingMethod] = None,
+                 time: Optional[str] = None, ctx: Optional[Context] = None, caller_ops=None):
+        method = method or NullCapturing()
+        spec = method.gpu_spec()
+        self.ctx = ctx or default_context()
+        self.state_shape = state.u.shape
+        d = L.frg_solve_desc()
+        self._keep = []
+        sch = state.scheme
+        d.dim = state.dim
+        d.p = state.ops.p
+        d.points = L.POINTS[sch.points]
+        d.flux = L.FLUX[sch.flux]
+        d.time_scheme = L.TIME[time or sch.time]
+        d.gamma = eq.gamma
+        m = state.mesh
+        xv = np.ascontiguousarray(m.x_vertices)
+        self._keep.append(xv)
+        d.x_vertices = L.dptr(xv)
+        if state.dim == 1:
+            d.nx, d.ny = m.n_elements, 1
+            d.x_left, d.x_right = m.x_left, m.x_right
+            d.bc[0] = _bc_struct(m.left_bc)
+            d.bc[1] = _bc_struct(m.right_bc)
+        else:
+            d.nx, d.ny = m.nx, m.ny
+            d.x_left, d.x_right, d.y_bottom, d.y_top = m.x_left, m.x_right, m.y_bottom, m.y_top
+            yv = np.ascontiguousarray(m.y_vertices)
+            self._keep.append(yv)
+            d.y_vertices = L.dptr(yv)
+            for k, bc in enumerate((m.left_bc, m.right_bc, m.bottom_bc, m.top_bc)):
+                d.bc[k] = _bc_struct(bc)
+            if m.solid is not None:
+                sol = np.ascontiguousarray(m.solid, dtype=np.uint8)
+                self._keep.append(sol)
+                d.solid = sol.ctypes.data_as(C.c_void_p)
+            if state.metrics is not None:
+                mt = L.frg_metrics2d()
+                for name in L._METRIC_FIELDS:
+                    a = np.asfortranarray(state.metrics[name], dtype=np.float64).ravel(order="F")
+                    a = np.ascontiguousarray(a)
+                    self._keep.append(a)
+                    setattr(mt, name, L.dptr(a))
+                self._keep.append(mt)
+                d.geometry = L.GEOM["metrics"]
+                d.metrics = C.pointer(mt)
+            elif state.wavy_amp is not None:
+                d.geometry = L.GEOM["wavy"]
+                d.wavy_amp = state.wavy_amp
+        if caller_ops is not None:
+            o = L.frg_operators()
+            o.p = caller_ops["p"] if isinstance(caller_ops, dict) else caller_ops.p
+            o.points = d.points
+            for name in ("xi", "w", "D", "l_L", "l_R", "gL_xi", "gR_xi", "V"):
+                src = caller_ops[name] if isinstance(caller_ops, dict) else getattr(
+                    caller_ops, "V_legendre" if name == "V" else name)
+                a = np.ascontiguousarray(np.asarray(src, dtype=np.float64).ravel(order="F"))
+                self._keep.append(a)
+                setattr(o, name, L.dptr(a))
+            self._keep.append(o)
+            d.ops = C.pointer(o)
+        d.method = L.METHOD[spec["method"]]
+        d.av_form = L.AV_FORM[spec["av_form"]]
+        d.kappa, d.s0_factor, d.eps_floor, d.c_av = (spec["kappa"], spec["s0_factor"],
+                                                    spec["eps_floor"], spec["c_av"])
+        self.desc = d
+        h = C.c_void_p()
+        L.check(L.load().frg_solve_create(self.ctx.handle, C.byref(d), C.byref(h)), self.ctx.handle,
+                "frg_solve_create")
+        self.handle = h
+        info = self.info()
+        self.ndof, self.nel = info["ndof"], info["nel"]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().frg_solve_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, code, what):
+        return L.check(code, self.ctx.handle, what)
+
+    def info(self) -> dict:
+        i = L.frg_solve_info()
+        self._chk(L.load().frg_solve_get_info(self.handle, C.byref(i)), "frg_solve_get_info")
+        return {"ndof": i.ndof, "nel": i.nel, "np": i.np, "neq": i.neq, "device_bytes": i.device_bytes,
+                "residual_evals": i.residual_evals, "steps": i.steps}
+
+    def upload(self, u: np.ndarray, t: float) -> None:
+        flat = np.ascontiguousarray(np.asarray(u, dtype=np.float64).ravel(order="F"))
+        self._chk(L.load().frg_upload_state(self.handle, L.dptr(flat), flat.size, float(t)), "upload")
+
+    def download(self):
+        flat = np.empty(self.ndof)
+        t = C.c_double()
+        self._chk(L.load().frg_download_state(self.handle, L.dptr(flat), flat.size, C.byref(t)), "download")
+        return flat.reshape(self.state_shape, order="F"), t.value
+
+    def residual(self) -> np.ndarray:
+        du = np.empty(self.ndof)
+        self._chk(L.load().frg_residual(self.handle, L.dptr(du), du.size), "frg_residual")
+        return du.reshape(self.state_shape, order="F")
+
+    def sense(self) -> np.ndarray:
+        s = np.empty(self.nel)
+        self._chk(L.load().frg_sense(self.handle, L.dptr(s), s.size), "frg_sense")
+        return s
+
+    def compute_dt(self, cfl: float) -> float:
+        dt = C.c_double()
+        self._chk(L.load().frg_compute_dt(self.handle, float(cfl), C.byref(dt)), "frg_compute_dt")
+        return dt.value
+
+    def step(self, dt: float) -> str:
+        st = C.c_int()
+        self._chk(L.load().frg_step(self.handle, float(dt), C.byref(st)), "frg_step")
+        return L.STATUS_SYMBOL[st.value]
+
+    def advance(self, t_final: float, cfl: float = 0.2, dt: Optional[float] = None,
+                max_steps: int = 10**7) -> dict:
+        r = L.frg_result()
+        self._chk(L.load().frg_advance(self.handle, float(t_final), float(cfl),
+                                       -1.0 if dt is None else float(dt), int(max_steps), C.byref(r)),
+                  "frg_advance")
+        return {"status": L.STATUS_SYMBOL[r.status], "n_steps": int(r.n_steps), "t": r.t}
+
+    def time_stages(self, nsteps: int, cfl: float = 0.2, dt: Optional[float] = None):
+        """Run nsteps steps with every stage kernel bracketed by CUDA events;
+        returns (mean stage-kernel ms per stage, result dict)."""
+        ms = np.zeros(3)
+        r = L.frg_result()
+        self._chk(L.load().frg_time_stages(self.handle, int(nsteps), float(cfl),
+                                           -1.0 if dt is None else float(dt), L.dptr(ms), C.byref(r)),
+                  "frg_time_stages")
+        return ms, {"status": L.STATUS_SYMBOL[r.status], "n_steps": int(r.n_steps), "t": r.t}
+
+
+def _solve_for(state, eq, method, time=None) -> GpuSolve:
+    method = method or NullCapturing()
+    spec = method.gpu_spec()
+    key = (tuple(sorted(spec.items())), time or state.scheme.time, state.scheme, eq.gamma)
+    s = state._gpu.get(key)
+    if s is None:
+        s = GpuSolve(state, eq, method, time=time)
+        state._gpu[key] = s
+    return s
+
+
+def residual_(du, state, eq, method: Optional[AbstractCapturingMethod] = None):
+    """residual!(du, state, eq, method) on the GPU."""
+    s = _solve_for(state, eq, method)
+    s.upload(state.u, state.t)
+    du[...] = s.residual()
+    return du
+
+
+def sense_(sigma, method, state, eq):
+    """sense!(sigma, method, u_work, state, eq): Persson element sensor."""
+    s = _solve_for(state, eq, method)
+    s.upload(state.u, state.t)
+    sigma[...] = s.sense()
+    return sigma
+
+
+def compute_dt(state, eq, cfl: float = 0.2) -> float:
+    s = _solve_for(state, eq, None)
+    s.upload(state.u, state.t)
+    return s.compute_dt(cfl)
+
+
+def _step(state, eq, method, dt, time):
+    s = _solve_for(state, eq, method, time)
+    s.upload(state.u, state.t)
+    status = s.step(dt)
+    state.u[...], state.t = s.download()
+    return status
+
+
+def ssp_rk3_step_(state, eq, method, dt: float) -> str:
+    """ssp_rk3_step! (SSP_RK3.jl:29-65, :135-164): 'ok' or 'diverged'."""
+    return _step(state, eq, method, dt, "ssp_rk3")
+
+
+def ssp_rk2_step_(state, eq, method, dt: float) -> str:
+    """ssp_rk2_step! (SSP_RK2.jl:14-68)."""
+    return _step(state, eq, method, dt, "ssp_rk2")
+
+
+def _run(state, eq, method, t_final, cfl, dt, max_steps, time):
+    s = _solve_for(state, eq, method, time)
+    s.upload(state.u, state.t)
+    r = s.advance(t_final, cfl=cfl, dt=dt, max_steps=max_steps)
+    state.u[...], state.t = s.download()
+    return r
+
+
+def ssp_rk3_(state, eq, method, t_final, cfl=0.2, dt=None, max_steps=10**7) -> dict:
+    """ssp_rk3!(state, eq, method, t_final; cfl, dt, max_steps)."""
+    return _run(state, eq, method, t_final, cfl, dt, max_steps, "ssp_rk3")
+
+
+def ssp_rk2_(state, eq, method, t_final, cfl=0.2, dt=None, max_steps=10**7) -> dict:
+    return _run(state, eq, method, t_final, cfl, dt, max_steps, "ssp_rk2")
+
+
+def integrate_(state, eq, method, t_final, cfl=0.2, dt=None, max_steps=10**7, time=None) -> dict:
+    """integrate!(state, eq, method, t_final; cfl, dt, max_steps, time)
+    (src/time/Integrate.jl:9-43)."""
+    tsym = time or state.scheme.time
+    if tsym not in ("ssp_rk3", "ssp_rk2"):
+        raise ValueError(f"Unknown time scheme {tsym} (use :ssp_rk3 or :ssp_rk2)")
+    return _run(state, eq, method, t_final, cfl, dt, max_steps, tsym)

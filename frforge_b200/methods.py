@@ -1,0 +1,161 @@
+"""Capturing-method hook surface and registry (src/capturing/Interfaces.jl,
+PerssonAV.jl, src/methods/Registry.jl, ScaledPersson.jl).
+
+A method is an object with the reference's six hooks.  The GPU library
+implements the default hooks, the Persson modal sensor and both dissipation
+forms; ``gpu_spec()`` turns a method into the solve descriptor fields.  A
+subclass that overrides a hook with host code has no device form: building
+its descriptor raises ``UnsupportedHookError`` instead of silently running
+something else.
+"""
+from __future__ import annotations
+
+from typing import Callable, Dict
+
+from ._lib import FRG_ERR_UNSUPPORTED_HOOK, UnsupportedHookError
+
+HOOKS = ("preprocess_state_", "extrapolate_interface_", "numerical_flux_method", "sense_",
+         "apply_dissipation_", "post_step_")
+
+
+class AbstractCapturingMethod:
+    """Hook defaults are identities (Interfaces.jl:43-92).  The GPU runs them
+    as part of the fused stage kernel; calling them on the host is not part
+    of the GPU path."""
+
+    def preprocess_state_(self, u_work, state, eq):
+        u_work[...] = state.u
+        return u_work
+
+    def extrapolate_interface_(self, traces, u_work, state, eq):
+        raise NotImplementedError("interface extrapolation runs inside the GPU stage kernel")
+
+    def numerical_flux_method(self, eq, uL, uR):
+        return None
+
+    def sense_(self, sigma, u_work, state, eq):
+        sigma[...] = 0.0
+        return sigma
+
+    def apply_dissipation_(self, du, sigma, u_work, state, eq):
+        return du
+
+    def post_step_(self, state, eq):
+        return None
+
+    # -- GPU descriptor ----------------------------------------------------
+    _gpu_base: tuple = ()
+
+    def gpu_spec(self) -> dict:
+        for base in type(self).__mro__:
+            if base in _GPU_CLASSES:
+                known = base
+                break
+        else:
+            raise UnsupportedHookError(FRG_ERR_UNSUPPORTED_HOOK,
+                                       f"{type(self).__name__} has no GPU implementation")
+        for h in HOOKS:
+            if getattr(type(self), h) is not getattr(known, h):
+                raise UnsupportedHookError(
+                    FRG_ERR_UNSUPPORTED_HOOK,
+                    f"{type(self).__name__}.{h} overrides a hook the GPU path cannot run")
+        return known._spec(self)
+
+    @staticmethod
+    def _spec(m) -> dict:
+        return {"method": "null", "av_form": "conservative_br0", "kappa": 4.0, "s0_factor": -4.0,
+                "eps_floor": 1e-16, "c_av": 0.0}
+
+
+class NullCapturing(AbstractCapturingMethod):
+    """Default method: no sensor, no artificial viscosity."""
+
+    def method_params(self):
+        return {"method": "null"}
+
+
+class PerssonSensor:
+    """Persson-Peraire modal sensor parameters (PerssonAV.jl:8-27)."""
+
+    def __init__(self, kappa=4.0, s0_factor=-4.0, eps_floor=1e-16):
+        self.kappa, self.s0_factor, self.eps_floor = float(kappa), float(s0_factor), float(eps_floor)
+
+
+class ElementArtificialViscosity:
+    """eps_e = c_av * sigma_e * (h_e/p) * lambda_e (PerssonAV.jl:30-49)."""
+
+    def __init__(self, c_av=0.1, av_form="conservative_br0"):
+        if av_form not in ("conservative_br0", "element_local_DD"):
+            raise ValueError(f"Unsupported av_form={av_form}")
+        self.c_av, self.av_form = float(c_av), av_form
+
+
+class PerssonAVMethod(AbstractCapturingMethod):
+    """Persson modal sensor + element AV (PerssonAV.jl:53-100); the code
+    default c_av is 0.1 (PerssonAV.jl:60, :72-77)."""
+
+    def __init__(self, kappa=4.0, s0_factor=-4.0, c_av=0.1, av_form="conservative_br0"):
+        self.sensor = PerssonSensor(kappa, s0_factor)
+        self.dissip = ElementArtificialViscosity(c_av, av_form)
+
+    def sense_(self, sigma, u_work, state, eq):  # runs on the GPU (see gpu.sense_)
+        raise NotImplementedError("the Persson sensor runs in the GPU stage kernel; use frforge_b200.sense_")
+
+    def apply_dissipation_(self, du, sigma, u_work, state, eq):
+        raise NotImplementedError("artificial viscosity runs in the GPU stage kernel")
+
+    def method_params(self):
+        return {"κ": self.sensor.kappa, "s0_factor": self.sensor.s0_factor,
+                "c_av": self.dissip.c_av, "av_form": self.dissip.av_form, "method": "persson_av"}
+
+    @staticmethod
+    def _spec(m) -> dict:
+        return {"method": "persson", "av_form": m.dissip.av_form, "kappa": m.sensor.kappa,
+                "s0_factor": m.sensor.s0_factor, "eps_floor": m.sensor.eps_floor,
+                "c_av": m.dissip.c_av}
+
+
+class ScaledPerssonMethod(AbstractCapturingMethod):
+    """Persson AV with c_av = 0.5 forwarding every hook to the inner method
+    (src/methods/ScaledPersson.jl:15-62)."""
+
+    def __init__(self, kappa=4.0, s0_factor=-4.0, c_av=0.5, av_form="conservative_br0"):
+        self.inner = PerssonAVMethod(kappa, s0_factor, c_av, av_form)
+
+    def method_params(self):
+        p = self.inner.method_params()
+        p["method"] = "scaled_persson"
+        p["note"] = "example inventable method; elevated c_av over baseline persson_av"
+        return p
+
+    @staticmethod
+    def _spec(m) -> dict:
+        return m.inner.gpu_spec()
+
+
+_GPU_CLASSES = (ScaledPerssonMethod, PerssonAVMethod, NullCapturing)
+
+# Method registry (Interfaces.jl:118-135, src/methods/Registry.jl:14-53)
+METHOD_REGISTRY: Dict[str, Callable[..., AbstractCapturingMethod]] = {
+    "null": lambda **kw: NullCapturing(),
+    "persson_av": lambda **kw: PerssonAVMethod(**kw),
+    "scaled_persson": lambda **kw: ScaledPerssonMethod(**kw),
+}
+
+
+def register_method(name: str, factory: Callable[..., AbstractCapturingMethod]) -> None:
+    METHOD_REGISTRY[str(name)] = factory
+
+
+def get_capturing_method(name: str, **kwargs) -> AbstractCapturingMethod:
+    if name not in METHOD_REGISTRY:
+        raise KeyError(f'Unknown capturing method "{name}". Known: {", ".join(sorted(METHOD_REGISTRY))}')
+    return METHOD_REGISTRY[name](**kwargs)
+
+
+def list_methods():
+    return sorted(METHOD_REGISTRY)
+
+
+def method_params(m) -> dict:
+    return m.method_params() if hasattr(m, "method_params") else {}

@@ -1,0 +1,213 @@
+/*
+ * frforge_cuda.h -- C ABI of the B200 (sm_100a) FR residual + SSP-RK library.
+ *
+ * This is the drop-in boundary for FRForge's hot path.  Each entry point
+ * names the Julia function it replaces (paths are relative to the FRForge
+ * source tree).  Conventions:
+ *   - every function returns an int status (frg_status); numerical outcomes
+ *     of a time integration (ok / diverged / max_steps) are reported in
+ *     frg_result.status exactly like the Symbol returned by ssp_rk3!
+ *     (src/time/SSP_RK3.jl:110-117); configuration errors map to
+ *     FRG_ERR_INVALID_ARG (Julia's ArgumentError, src/scheme/SchemeConfig.jl:26-29);
+ *   - arrays use FRForge's Julia layout: u[j,e,c] (1D) / u[i,j,e,c] (2D),
+ *     column-major, FP64 -- so upload/download are plain copies;
+ *   - the library owns all device memory of a solve; host buffers are owned
+ *     by the caller and only read/written during the call;
+ *   - calls on one solve are serialised on that solve's CUDA stream; one
+ *     frg_ctx per host thread.
+ */
+#ifndef FRFORGE_CUDA_H
+#define FRFORGE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FRG_ABI_VERSION 1
+#define FRG_MAX_NP 6 /* P <= 5 */
+
+/* Status codes.  Numerical statuses mirror :ok / :diverged / :max_steps
+   (src/time/SSP_RK3.jl:44-64, :110-117). */
+typedef enum {
+  FRG_OK = 0,
+  FRG_DIVERGED = 1,
+  FRG_MAX_STEPS = 2,
+  FRG_ERR_INVALID_ARG = -1,      /* ArgumentError in the reference */
+  FRG_ERR_UNSUPPORTED_HOOK = -2, /* a capturing hook with no GPU implementation */
+  FRG_ERR_OOM = -3,              /* device allocation / admission budget */
+  FRG_ERR_CUDA = -4,             /* CUDA runtime failure; see frg_last_error */
+  FRG_ERR_TIMEOUT = -5,          /* bounded device wait gave up */
+  FRG_ERR_STATE = -6             /* call order (e.g. no state uploaded) */
+} frg_status;
+
+/* Scheme axes, src/scheme/SchemeConfig.jl:15-31 */
+enum { FRG_POINTS_GL = 0, FRG_POINTS_GLL = 1 };
+enum { FRG_FLUX_RUSANOV = 0, FRG_FLUX_HLLC = 1 };
+enum { FRG_TIME_SSP_RK3 = 0, FRG_TIME_SSP_RK2 = 1 };
+
+/* Boundary conditions, src/mesh/BoundaryConditions.jl:9-134.  XSPLIT is the
+   GhostStateBC shape used by the double-Mach case
+   (src/verification/Cases2D_Optional.jl:72-84): ghost = state for
+   x < x0 + (s0 + s1*t)/sdiv, else (mode 0) the reflected interior state or
+   (mode 1) state_b. */
+enum {
+  FRG_BC_PERIODIC = 0,
+  FRG_BC_TRANSMISSIVE = 1,
+  FRG_BC_DIRICHLET = 2,
+  FRG_BC_REFLECTING = 3,
+  FRG_BC_XSPLIT = 4
+};
+
+/* Capturing methods: NullCapturing (src/capturing/Interfaces.jl:21-26) and
+   PerssonAVMethod (src/capturing/PerssonAV.jl:53-77); scaled_persson
+   (src/methods/ScaledPersson.jl) is PERSSON with c_av = 0.5. */
+enum { FRG_METHOD_NULL = 0, FRG_METHOD_PERSSON = 1 };
+enum { FRG_AV_BR0 = 0, FRG_AV_LOCAL_DD = 1 };
+
+/* Geometry (2D): affine Cartesian mesh (build_mesh_metrics,
+   src/mesh/MeshMetrics2D.jl:82-218), analytic wavy map
+   (build_mesh_metrics_analytic_wavy, :327-442), or caller metrics. */
+enum { FRG_GEOM_AFFINE = 0, FRG_GEOM_WAVY = 1, FRG_GEOM_METRICS = 2 };
+
+typedef struct {
+  int kind; /* FRG_BC_* */
+  int mode; /* XSPLIT: 0 reflect interior, 1 state_b */
+  double state[4];
+  double state_b[4];
+  double x0, s0, s1, sdiv;
+} frg_bc;
+
+/* Reference-element tables of FROperators (src/fr/Operators.jl:62-77).
+   Matrices are np x np column-major (Julia layout). */
+typedef struct {
+  int p;
+  int points;
+  const double* xi;    /* np */
+  const double* w;     /* np */
+  const double* D;     /* np*np, D[i + np*k] = D[i,k] */
+  const double* l_L;   /* np */
+  const double* l_R;   /* np */
+  const double* gL_xi; /* np */
+  const double* gR_xi; /* np */
+  const double* V;     /* np*np Legendre Vandermonde */
+} frg_operators;
+
+/* Per-solve metrics (MeshMetrics2D, src/mesh/MeshMetrics2D.jl:15-39), used
+   with FRG_GEOM_METRICS.  SP fields are [np,np,nel]; face fields [np,nel]. */
+typedef struct {
+  const double *x_xi, *x_eta, *y_xi, *y_eta, *J;
+  const double *nx_W, *ny_W, *sJ_W, *nx_E, *ny_E, *sJ_E;
+  const double *nx_S, *ny_S, *sJ_S, *nx_N, *ny_N, *sJ_N;
+  const double* h_char; /* [nel] */
+} frg_metrics2d;
+
+/* Solve descriptor: SchemeConfig + Mesh1D/Mesh2D + metrics + method params. */
+typedef struct {
+  int dim; /* 1 or 2 */
+  int p;
+  int points;      /* FRG_POINTS_* */
+  int flux;        /* FRG_FLUX_* */
+  int time_scheme; /* FRG_TIME_* */
+  double gamma;
+  int nx, ny; /* 1D: nx = n_elements, ny = 1 */
+  double x_left, x_right, y_bottom, y_top;
+  const double* x_vertices; /* optional nx+1 (overrides x_left/x_right) */
+  const double* y_vertices; /* optional ny+1 */
+  frg_bc bc[4];             /* left, right, bottom, top (1D: left, right) */
+  const unsigned char* solid; /* optional [nel] solid-element mask (2D) */
+  int geometry;               /* FRG_GEOM_* (2D) */
+  double wavy_amp;
+  const frg_metrics2d* metrics; /* FRG_GEOM_METRICS */
+  const frg_operators* ops;     /* optional caller tables (NULL: built here) */
+  int method;                   /* FRG_METHOD_* */
+  int av_form;                  /* FRG_AV_* */
+  double kappa, s0_factor, eps_floor, c_av;
+} frg_solve_desc;
+
+typedef struct {
+  int status; /* FRG_OK / FRG_DIVERGED / FRG_MAX_STEPS */
+  int64_t n_steps;
+  double t;
+} frg_result;
+
+typedef struct {
+  size_t ndof;   /* state length (doubles) */
+  int nel, np, neq;
+  size_t device_bytes; /* HBM held by this solve */
+  int64_t residual_evals; /* residual (stage) evaluations so far */
+  int64_t steps;          /* completed time steps so far */
+} frg_solve_info;
+
+typedef struct frg_ctx frg_ctx;
+typedef struct frg_solve frg_solve;
+
+/* ---- library / context ---------------------------------------------- */
+int frg_abi_version(void);
+const char* frg_version(void);
+const char* frg_status_string(int status);
+
+/* Host construction of FROperators: replaces build_operators
+   (src/fr/Operators.jl:85-104) for callers without their own tables.  Any
+   output pointer may be NULL.  Matrices are column-major. */
+int frg_build_operators(int p, int points, double* xi, double* w, double* D,
+                        double* l_L, double* l_R, double* gL_xi, double* gR_xi,
+                        double* gL, double* gR, double* V);
+
+int frg_ctx_create(int device, frg_ctx** out);
+int frg_ctx_destroy(frg_ctx* ctx);
+const char* frg_last_error(const frg_ctx* ctx);
+/* The cudaStream_t every solve of this context is launched on (for event
+   timing and interop); no reference counterpart. */
+int frg_ctx_get_stream(frg_ctx* ctx, void** stream);
+
+/* ---- single solve ------------------------------------------------------ */
+/* allocate_state + build_mesh_metrics + method selection
+   (src/solvestate/SolutionState2D.jl:137-160, SolutionState.jl:25-39) */
+int frg_solve_create(frg_ctx* ctx, const frg_solve_desc* desc, frg_solve** out);
+int frg_solve_destroy(frg_solve* s);
+int frg_solve_get_info(const frg_solve* s, frg_solve_info* info);
+
+/* state.u / state.t upload and download (copies, Julia layout) */
+int frg_upload_state(frg_solve* s, const double* u, size_t n, double t);
+int frg_download_state(frg_solve* s, double* u, size_t n, double* t);
+
+/* residual!(du, state, eq, method): src/fr/Residual.jl:161-214 (1D),
+   src/fr/Residual2D.jl:131-416 (2D), including the sense! /
+   apply_dissipation! hooks of the method.  du is a host array of n doubles. */
+int frg_residual(frg_solve* s, double* du, size_t n);
+
+/* sense! (src/capturing/PerssonAV.jl:116-135, PerssonAV2D.jl:20-59): the
+   element sensor sigma of the current state; sigma has nel entries. */
+int frg_sense(frg_solve* s, double* sigma, size_t nel);
+
+/* compute_dt(state, eq; cfl): src/time/SSP_RK3.jl:8-24 (1D), :126-133 (2D) */
+int frg_compute_dt(frg_solve* s, double cfl, double* dt);
+
+/* ssp_rk3_step! / ssp_rk2_step! with the given dt (src/time/SSP_RK3.jl:29-65,
+   :135-164; src/time/SSP_RK2.jl:14-68).  *step_status receives FRG_OK or
+   FRG_DIVERGED. */
+int frg_step(frg_solve* s, double dt, int* step_status);
+
+/* integrate! / ssp_rk3! / ssp_rk2! (src/time/Integrate.jl:9-43,
+   src/time/SSP_RK3.jl:75-118, :166-211, src/time/SSP_RK2.jl:70-132):
+   advance to t_final with the CFL dt (fixed_dt <= 0) or a fixed dt; the last
+   step is clipped to t_final; max_steps caps the step count.  The whole loop
+   runs on the device (CUDA graphs of several steps); the host only polls the
+   device status word between graph launches. */
+int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt,
+                int64_t max_steps, frg_result* out);
+
+/* Instrumented frg_advance for profiling (no reference counterpart): runs
+   nsteps steps with direct launches and times every stage kernel with CUDA
+   events on the solve's stream; stage_ms[k] = mean duration (ms) of the
+   stage-(k+1) kernel, k = 0..2 (stage 3 unused for SSP-RK2). */
+int frg_time_stages(frg_solve* s, int64_t nsteps, double cfl, double fixed_dt,
+                    double* stage_ms, frg_result* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
