@@ -1,0 +1,304 @@
+"""Benchmark: FP64 DOF-stage updates/s of the FR residual + SSP-RK3 path.
+
+Workload (default): 512^2 quads, GL P=3, HLLC, SSP-RK3, Persson AV (BR0,
+c_av 0.1), transmissive, CFL 0.1, seeded four-quadrant IC (see
+frforge_b200/workloads.py).  A "step" is one SSP-RK3 step = 3 stage
+evaluations over all 512^2 x 16 x 4 = 16.8M degrees of freedom.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours: value = DOF-stage/s with the state resident in HBM, timed with CUDA
+events on the library's stream (max over ranks); e2e = the same metric through
+the public C ABI with pinned host buffers (state upload + K steps + download
+inside the timed region); roofline of the fused stage kernel from CUDA events
+around every stage launch; cpu_baseline = the C oracle on a bounded sample.
+reference: the reference algorithm on the host cores (the C oracle port, all
+threads), each step one SSP-RK3 step of a 128^2 sample of the workload.
+Multi-GPU: replicas only (each rank runs its own solve, no data exchange).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 DOF-stage updates/s on 1 B200; batched solves/s + p99 latency vs plain"
+UNIT = "DOF-stage/s"
+# algorithmic HBM bytes per DOF per stage (SSP-RK3: 16, 24, 24 -> 64/3 avg)
+STAGE_BYTES = (16.0, 24.0, 24.0)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.15)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def oracle_rate(n: int, steps: int, threads: int, min_seconds: float = 0.0):
+    """DOF-stage/s of the C oracle on an n x n sample of the c3 workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from frforge_b200.workloads import C3, four_quadrant_ic, four_quadrant_states
+
+    O.set_threads(threads)
+    s = O.OracleSolver.two_d(p=C3.p, nx=n, ny=n, bcs=[O.make_bc("transmissive")] * 4, flux=C3.flux,
+                             method="persson", c_av=C3.c_av)
+    x, y = s.coords()
+    s.set_state(four_quadrant_ic(x, y, four_quadrant_states(C3.seed, C3.jump_scale)))
+    ndof = s.ndof
+    s.integrate(1e9, cfl=C3.cfl, max_steps=1)  # warm the caches / thread pool
+    done = 0
+    t0 = time.perf_counter()
+    while done < steps or (time.perf_counter() - t0) < min_seconds:
+        r = s.integrate(1e9, cfl=C3.cfl, max_steps=1)
+        if r["status"] == "diverged":
+            raise RuntimeError("oracle sample diverged")
+        done += 1
+    dt = time.perf_counter() - t0
+    return 3 * ndof * done / dt, done, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n = 128
+    oracle_rate(n, max(1, args.warmup), threads)
+    rate, done, dt = oracle_rate(n, args.steps, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded four-quadrant Riemann IC)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"one SSP-RK3 step of a {n}^2 sample of the workload per step "
+                                   f"(same P, flux, method, IC); C oracle, OpenMP {threads} threads"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def workload_config(args):
+    return {"workload": "2D Euler 512x512 quads, GL P=3, HLLC, SSP-RK3, Persson AV (BR0, c_av=0.1), "
+                        "transmissive, CFL 0.1, seeded four-quadrant Riemann IC",
+            "elements": 512 * 512, "p": 3, "dof": 512 * 512 * 16 * 4, "stages_per_step": 3,
+            "l2": "inputs larger than L2 (3 x 134 MB state buffers)", "parallelism": f"replicas{args.gpus}"}
+
+
+def traffic_per_launch():
+    """dram bytes per stage launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "stage2d_c3_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("dram_bytes_per_launch_full_c3")
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import frforge_b200 as F
+    from frforge_b200.workloads import C3
+
+    ctx = F.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", local))
+    st, method = C3.build(F)
+    solve = F.GpuSolve(st, F.Euler2D(1.4), method, ctx=ctx)
+    ndof = solve.ndof
+    u_host = torch.empty(ndof, dtype=torch.float64, pin_memory=True)
+    u_host.numpy()[:] = st.u.ravel(order="F")
+    u_out = torch.empty(ndof, dtype=torch.float64, pin_memory=True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (untimed)
+    solve.upload(u_host.numpy().reshape(st.u.shape, order="F"), 0.0)
+    r = solve.advance(1e9, cfl=C3.cfl, max_steps=max(3, args.warmup))
+    if r["status"] == "diverged":
+        raise RuntimeError("warm-up diverged")
+
+    # ---- device-resident timed region: K steps, events on the library stream
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        r = solve.advance(1e9, cfl=C3.cfl, max_steps=args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    if r["status"] != "max_steps" or r["n_steps"] != args.steps:
+        raise RuntimeError(f"timed run ended early: {r}")
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * 3 * ndof / (ms_max * 1e-3)
+
+    # ---- stage-kernel roofline: CUDA events around every stage launch
+    nst = max(3, min(args.steps, 30))
+    stage_ms, _ = solve.time_stages(nst, cfl=C3.cfl)
+    alg_bytes = sum(STAGE_BYTES) / 3.0 * ndof  # per launch (average over the 3 stages)
+    mean_stage_ms = float(np.mean(stage_ms))
+    achieved_gbs = alg_bytes / (mean_stage_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # ---- end-to-end through the public C ABI with pinned host buffers
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    solve.upload_ptr(u_host.data_ptr(), 0.0)
+    r2 = solve.advance(1e9, cfl=C3.cfl, max_steps=args.steps)
+    solve.download_ptr(u_out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * 3 * ndof / (float(t.item()) * 1e-3)
+    if not np.all(np.isfinite(u_out.numpy())) or r2["status"] != "max_steps":
+        raise RuntimeError("e2e run produced a non-finite state")
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            rate, done, dt = oracle_rate(128, 2, threads, min_seconds=10.0)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{done} SSP-RK3 steps of a 128^2 sample of the workload (same P, flux, "
+                             f"method, IC) in {dt:.1f} s; C oracle, OpenMP {threads} threads"}
+        tr = traffic_per_launch()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded four-quadrant Riemann IC)", "config": workload_config(args),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ndof * 8 / args.steps,
+                    "d2h_bytes_per_step": ndof * 8 / args.steps,
+                    "note": "public C ABI: frg_upload_state (pinned host) + frg_advance(K) + "
+                            "frg_download_state inside the timed region"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_gbs / peak, "traffic": tr,
+                         "kernel": "frg::stage2d_kernel<4,HLLC,BR0>",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "stage_ms": [float(x) for x in stage_ms], "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": args.steps * 5,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -123,11 +123,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           double su = 0.0, sg = 0.0;
+          const double vc = sU[(sA * NEQ + c) * NP + NP / 2];
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double v = sU[(sA * NEQ + c) * NP + i];
             su += ops.lR[i] * v;
-            if (kBR0) sg += ops.lRD[i] * v;
+            if (kBR0) sg += ops.lRD[i] * (v - vc);
           }
           uA[c] = su;
           gA[c] = sg;
@@ -137,11 +138,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           double su = 0.0, sg = 0.0;
+          const double vc = sU[(sB * NEQ + c) * NP + NP / 2];
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double v = sU[(sB * NEQ + c) * NP + i];
             su += ops.lL[i] * v;
-            if (kBR0) sg += ops.lLD[i] * v;
+            if (kBR0) sg += ops.lLD[i] * (v - vc);
           }
           uB[c] = su;
           gB[c] = sg;
@@ -186,13 +188,15 @@ __global__ void __launch_bounds__(256)
     for (int idx = tid; idx < TX * NEQ; idx += nthr) {
       const int c = idx % NEQ, o = idx / NEQ, s = o + 1;
       if (!sOwn[s]) continue;
+      // shifted lines: Dt 1 = -(gL + gR), DtD 1 = DD 1 = 0 (exact identities)
       double Fl[NP], Ul[NP];
+      const double fc = sF[(o * NEQ + c) * NP + NP / 2], uc = sU[(s * NEQ + c) * NP + NP / 2];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        Fl[k] = sF[(o * NEQ + c) * NP + k];
-        Ul[k] = sU[(s * NEQ + c) * NP + k];
+        Fl[k] = sF[(o * NEQ + c) * NP + k] - fc;
+        Ul[k] = sU[(s * NEQ + c) * NP + k] - uc;
       }
-      const double fL = sFace[o * 8 + c], fR = sFace[(o + 1) * 8 + c];
+      const double fL = sFace[o * 8 + c] - fc, fR = sFace[(o + 1) * 8 + c] - fc;
       const double gLh = kBR0 ? sFace[o * 8 + 4 + c] : 0.0;
       const double gRh = kBR0 ? sFace[(o + 1) * 8 + 4 + c] : 0.0;
       const double J = sJ[s], rJ = 1.0 / J;

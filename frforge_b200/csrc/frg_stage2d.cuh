@@ -228,16 +228,19 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       const int eA = sEl[sA], eB = sEl[sB];
       double uA[4], uB[4], gA[4], gB[4];
       // traces: A's east/north face, B's west/south face
+      // g traces use l^T D, whose entries sum to zero: shifting the line by
+      // one of its values removes the cancellation of large terms exactly.
       if (eA >= 0) {
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           const double* a = sU + (sA * NEQ + c) * NP2;
+          const double vc = vert ? a[NP / 2 + NP * q] : a[q + NP * (NP / 2)];
           double su = 0.0, sg = 0.0;
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double v = vert ? a[i + NP * q] : a[q + NP * i];
             su += ops.lR[i] * v;
-            if (kBR0) sg += ops.lRD[i] * v;
+            if (kBR0) sg += ops.lRD[i] * (v - vc);
           }
           uA[c] = su;
           gA[c] = sg;
@@ -247,12 +250,13 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           const double* b = sU + (sB * NEQ + c) * NP2;
+          const double vc = vert ? b[NP / 2 + NP * q] : b[q + NP * (NP / 2)];
           double su = 0.0, sg = 0.0;
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
             const double v = vert ? b[i + NP * q] : b[q + NP * i];
             su += ops.lL[i] * v;
-            if (kBR0) sg += ops.lLD[i] * v;
+            if (kBR0) sg += ops.lLD[i] * (v - vc);
           }
           uB[c] = su;
           gB[c] = sg;
@@ -385,15 +389,18 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         continue;
       }
       const double* Uo = sU + (s * NEQ + c) * NP2;
+      // Dt 1 = -(gL + gR) and DtD 1 = DD 1 = 0: every line is shifted by its
+      // middle value so the folded operators never cancel large terms.
       double Fl[NP], Ul[NP];
+      const double fc = Fo[NP / 2 + NP * j], uc = Uo[NP / 2 + NP * j];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        Fl[k] = Fo[k + NP * j];
-        Ul[k] = Uo[k + NP * j];
+        Fl[k] = Fo[k + NP * j] - fc;
+        Ul[k] = Uo[k + NP * j] - uc;
       }
       const int fW = oy * (TX + 1) + ox;
-      const double fhW = sFV[(fW * NP + j) * 8 + c];
-      const double fhE = sFV[((fW + 1) * NP + j) * 8 + c];
+      const double fhW = sFV[(fW * NP + j) * 8 + c] - fc;
+      const double fhE = sFV[((fW + 1) * NP + j) * 8 + c] - fc;
       const double ghW = kBR0 ? sFV[(fW * NP + j) * 8 + 4 + c] : 0.0;
       const double ghE = kBR0 ? sFV[((fW + 1) * NP + j) * 8 + 4 + c] : 0.0;
       const double jx = sJx[s];
@@ -441,14 +448,15 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       }
       const double* Uo = sU + (s * NEQ + c) * NP2;
       double Gl[NP], Ul[NP];
+      const double gc = Go[i + NP * (NP / 2)], uc = Uo[i + NP * (NP / 2)];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        Gl[k] = Go[i + NP * k];
-        Ul[k] = Uo[i + NP * k];
+        Gl[k] = Go[i + NP * k] - gc;
+        Ul[k] = Uo[i + NP * k] - uc;
       }
       const int fS = oy * TX + ox;
-      const double fhS = sFH[(fS * NP + i) * 8 + c];
-      const double fhN = sFH[((fS + TX) * NP + i) * 8 + c];
+      const double fhS = sFH[(fS * NP + i) * 8 + c] - gc;
+      const double fhN = sFH[((fS + TX) * NP + i) * 8 + c] - gc;
       const double ghS = kBR0 ? sFH[(fS * NP + i) * 8 + 4 + c] : 0.0;
       const double ghN = kBR0 ? sFH[((fS + TX) * NP + i) * 8 + 4 + c] : 0.0;
       const double jy = sJy[s];

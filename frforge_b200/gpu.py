@@ -179,6 +179,18 @@ class GpuSolve:
         flat = np.ascontiguousarray(np.asarray(u, dtype=np.float64).ravel(order="F"))
         self._chk(L.load().frg_upload_state(self.handle, L.dptr(flat), flat.size, float(t)), "upload")
 
+    def upload_ptr(self, host_ptr: int, t: float) -> None:
+        """Upload ndof doubles from a raw host address (e.g. pinned memory)."""
+        self._chk(L.load().frg_upload_state(self.handle, C.cast(host_ptr, L._dp), self.ndof, float(t)),
+                  "upload")
+
+    def download_ptr(self, host_ptr: int) -> float:
+        """Download the state to a raw host address; returns its time."""
+        t = C.c_double()
+        self._chk(L.load().frg_download_state(self.handle, C.cast(host_ptr, L._dp), self.ndof,
+                                              C.byref(t)), "download")
+        return t.value
+
     def download(self):
         flat = np.empty(self.ndof)
         t = C.c_double()

@@ -1,0 +1,119 @@
+"""Seeded synthetic workloads (no public suite is involved).
+
+All draws come from one SplitMix64 stream (Steele, Lea & Flood 2014) in a
+fixed order, default seed 20261203, so the oracle, the GPU and the CPU
+baseline see identical inputs.
+
+* c1: 1D Euler, 256 elements on [0,1], GL P=3, Rusanov, SSP-RK3, Persson AV
+  (c_av 0.1, BR0), transmissive; two-state Riemann IC at x=0.5 with left then
+  right (rho, u, p) drawn rho~U[0.1,1], u~U[-0.5,0.5], p~U[0.1,1]; CFL 0.1.
+* c2: 2D periodic [0,1]^2, 128^2 affine quads, GL P=4, Rusanov, SSP-RK3,
+  Persson AV; rho = 1 + 0.2 sin(2 pi (x+y) + phi), phi~U[0,2pi), u=v=p=1.
+* c3: 2D [0,1]^2, 512^2 quads, GL P=3, HLLC, SSP-RK3, Persson AV (c_av 0.1,
+  BR0), transmissive, CFL 0.1; four-quadrant piecewise-constant IC split at
+  (0.5, 0.5) with the quadrant rule of riemann2d_ic
+  (src/verification/Cases2D_Riemann.jl:33-51).  The four (rho,u,v,p) states
+  are drawn rho~U[0.1,1.5], u,v~U[-0.8,0.8], p~U[0.05,1.5] in the order
+  ne, nw, sw, se, and then each state's deviation from the mean of the four
+  is scaled by ``jump_scale`` = 0.25: with the unscaled draws the reference
+  scheme itself (P=3 FR + HLLC + Persson AV, no positivity limiter) reaches
+  negative density and returns :diverged within 40 steps for every seed
+  tried, which would leave nothing to time.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Iterator, List, Tuple
+
+import numpy as np
+
+DEFAULT_SEED = 20261203
+
+
+def splitmix64(seed: int) -> Iterator[float]:
+    """Uniform doubles in [0, 1) from SplitMix64 (53-bit mantissa)."""
+    state = seed & 0xFFFFFFFFFFFFFFFF
+    while True:
+        state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        z ^= z >> 31
+        yield (z >> 11) * (1.0 / 9007199254740992.0)
+
+
+def uniform(g: Iterator[float], lo: float, hi: float) -> float:
+    return lo + (hi - lo) * next(g)
+
+
+def four_quadrant_states(seed: int = DEFAULT_SEED, jump_scale: float = 0.25) -> List[Tuple[float, ...]]:
+    g = splitmix64(seed)
+    st = []
+    for _ in range(4):
+        st.append(np.array([uniform(g, 0.1, 1.5), uniform(g, -0.8, 0.8), uniform(g, -0.8, 0.8),
+                            uniform(g, 0.05, 1.5)]))
+    m = sum(st) / 4.0
+    return [tuple(m + jump_scale * (s - m)) for s in st]
+
+
+def four_quadrant_ic(X, Y, states, gamma=1.4, x0=0.5, y0=0.5) -> np.ndarray:
+    """Conserved state [..., 4] of the four-quadrant rule (riemann2d_ic)."""
+    ne, nw, sw, se = [np.asarray(s) for s in states]
+    P = np.where(((X >= x0) & (Y >= y0))[..., None], ne,
+                 np.where(((X < x0) & (Y >= y0))[..., None], nw,
+                          np.where(((X < x0) & (Y < y0))[..., None], sw, se)))
+    r, u, v, p = P[..., 0], P[..., 1], P[..., 2], P[..., 3]
+    E = p / (gamma - 1.0) + 0.5 * r * (u * u + v * v)
+    return np.stack([r, r * u, r * v, E], axis=-1)
+
+
+def two_state_1d(seed: int = DEFAULT_SEED):
+    g = splitmix64(seed)
+    L = (uniform(g, 0.1, 1.0), uniform(g, -0.5, 0.5), uniform(g, 0.1, 1.0))
+    R = (uniform(g, 0.1, 1.0), uniform(g, -0.5, 0.5), uniform(g, 0.1, 1.0))
+    return L, R
+
+
+@dataclass
+class Workload2D:
+    name: str
+    n: int
+    p: int
+    flux: str
+    method: str
+    c_av: float
+    periodic: bool
+    cfl: float
+    steps: int
+    seed: int = DEFAULT_SEED
+    jump_scale: float = 0.25
+
+    @property
+    def ndof(self) -> int:
+        return self.n * self.n * (self.p + 1) ** 2 * 4
+
+    def build(self, F):
+        """(state, method) for the frforge_b200 module F, IC filled in."""
+        bc = F.PeriodicBC if self.periodic else F.TransmissiveBC
+        mesh = F.Mesh2D(0.0, 1.0, 0.0, 1.0, self.n, self.n, bc(), bc(), bc(), bc())
+        ops = F.build_operators(self.p)
+        st = F.allocate_state(mesh, ops, 4, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+        X, Y = mesh.physical_coords(ops)
+        st.u[...] = self.initial_state(X, Y)
+        m = F.PerssonAVMethod(c_av=self.c_av) if self.method == "persson_av" else F.NullCapturing()
+        return st, m
+
+    def initial_state(self, X, Y) -> np.ndarray:
+        if self.name == "c2":
+            g = splitmix64(self.seed)
+            phi = uniform(g, 0.0, 2 * math.pi)
+            r = 1.0 + 0.2 * np.sin(2 * math.pi * (X + Y) + phi)
+            one = np.ones_like(r)
+            return np.stack([r, r, r, one / 0.4 + 0.5 * r * 2.0], axis=-1)
+        return four_quadrant_ic(X, Y, four_quadrant_states(self.seed, self.jump_scale))
+
+
+C2 = Workload2D("c2", 128, 4, "rusanov", "persson_av", 0.1, True, 0.1, 500)
+C3 = Workload2D("c3", 512, 3, "hllc", "persson_av", 0.1, False, 0.1, 1000)
+WORKLOADS = {"c2": C2, "c3": C3}

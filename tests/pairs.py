@@ -95,9 +95,10 @@ def pair_1d(p=3, nel=32, points="gl", flux="rusanov", time="ssp_rk3", method="nu
     return orc, state, solve
 
 
-def four_quadrant_state(orc, seed=20261203, x0=0.5, y0=0.5, states=None):
+def four_quadrant_state(orc, seed=20261203, x0=0.5, y0=0.5, states=None, jump_scale=1.0):
     """Seeded four-quadrant Riemann IC (riemann2d_ic quadrant rule,
-    Cases2D_Riemann.jl:33-51); draws in the order ne, nw, sw, se."""
+    Cases2D_Riemann.jl:33-51); draws in the order ne, nw, sw, se; each state's
+    deviation from the mean of the four is scaled by jump_scale."""
     if states is None:
         g = splitmix64(seed)
         states = []
@@ -106,7 +107,9 @@ def four_quadrant_state(orc, seed=20261203, x0=0.5, y0=0.5, states=None):
             u = -0.8 + 1.6 * next(g)
             v = -0.8 + 1.6 * next(g)
             p = 0.05 + 1.45 * next(g)
-            states.append((r, u, v, p))
+            states.append(np.array((r, u, v, p)))
+        m = sum(states) / 4.0
+        states = [tuple(m + jump_scale * (s - m)) for s in states]
     x, y = orc.coords()
     ne, nw, sw, se = [np.array(s) for s in states]
     P = np.where(((x >= x0) & (y >= y0))[..., None], ne,

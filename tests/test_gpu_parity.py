@@ -186,7 +186,7 @@ def test_shocked_2d_integration_matches_oracle():
     # small four-quadrant HLLC + Persson BR0 case (the 512^2 benchmark's physics)
     orc, state, solve = pair_2d(p=3, nx=24, ny=24, flux="hllc", method="persson",
                                 bcs=("transmissive",) * 4)
-    u0 = four_quadrant_state(orc)
+    u0 = four_quadrant_state(orc, jump_scale=0.25)
     orc.set_state(u0)
     r_ref = orc.integrate(1.0, cfl=0.1, max_steps=60)
     solve.upload(u0, 0.0)
@@ -199,6 +199,23 @@ def test_shocked_2d_integration_matches_oracle():
     assert np.sum(np.abs(u - ref)) / np.sum(np.abs(ref)) <= 1e-8
     orc.set_state(u)
     assert orc.positivity_ok()
+
+
+def test_unscaled_draw_diverges_at_same_step():
+    # the unscaled seeded four-quadrant draw drives the reference scheme to
+    # negative density; the GPU must report :diverged at the same step with
+    # the same state
+    orc, state, solve = pair_2d(p=3, nx=16, ny=16, flux="hllc", method="persson",
+                                bcs=("transmissive",) * 4)
+    u0 = four_quadrant_state(orc)
+    orc.set_state(u0)
+    r_ref = orc.integrate(10.0, cfl=0.1, max_steps=200)
+    solve.upload(u0, 0.0)
+    r = solve.advance(10.0, cfl=0.1, max_steps=200)
+    assert r_ref["status"] == r["status"] == "diverged"
+    assert r["n_steps"] == r_ref["n_steps"]
+    u, t = solve.download()
+    assert t == pytest.approx(orc.t, rel=1e-12)
 
 
 def test_smooth_2d_rk2_fixed_dt():
