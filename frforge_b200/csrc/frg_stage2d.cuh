@@ -3,7 +3,8 @@
 // One CTA owns a TX x TY tile of elements and stages the tile plus a
 // one-element halo ring (no corners) of the stage input in shared memory.
 // Everything a stage needs happens on chip:
-//   P0  load u (tile + halo) and the element viscosities eps (tile + halo)
+//   P0  cp.async prefetch of u_s (tile + halo) and, as a second commit group
+//       that lands while P1-P4 compute, the step-start state u0 of the tile
 //   P1  physical fluxes -> contravariant F~, G~ at every own solution point
 //       (Residual2D.jl:342-352)
 //   P2  every face point of the tile once: u traces of both sides
@@ -21,6 +22,10 @@
 //       SSP_RK3.jl:126-133) as one atomic max per CTA.
 // Halo values come from the neighbouring tiles' own loads, so they are
 // L2 hits; DRAM traffic per stage is the algorithmic u_s + u0 + u_out.
+//
+// Shared-memory blocks use odd strides (in doubles) between elements and
+// lanes walk over elements first, so a warp's 8-byte accesses spread over
+// all banks.
 #pragma once
 
 #include "frg_device.cuh"
@@ -29,15 +34,15 @@ namespace frg {
 
 template <int NP>
 struct Tile2D;
-// Tile shapes (elements).  Chosen so a CTA's shared memory lets 2 CTAs
-// reside per SM for P <= 4.
+// Tile shapes (elements): two CTAs of 256 threads reside per SM (register
+// bound at 128/thread), so each tile's shared memory stays under ~113 KB.
 template <>
 struct Tile2D<2> {
-  static constexpr int TX = 16, TY = 8;
+  static constexpr int TX = 8, TY = 8;
 };
 template <>
 struct Tile2D<3> {
-  static constexpr int TX = 8, TY = 8;
+  static constexpr int TX = 8, TY = 6;
 };
 template <>
 struct Tile2D<4> {
@@ -49,26 +54,30 @@ struct Tile2D<5> {
 };
 template <>
 struct Tile2D<6> {
-  static constexpr int TX = 4, TY = 4;
+  static constexpr int TX = 4, TY = 3;
 };
+
+constexpr int odd_up(int n) { return (n % 2) ? n : n + 1; }
 
 template <int NP, int TX, int TY>
 struct Smem2D {
   static constexpr int NEQ = 4, NP2 = NP * NP;
   static constexpr int BX = TX + 2, BY = TY + 2, NSLOT = BX * BY, NOWN = TX * TY;
   static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
+  static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
   // doubles
-  static constexpr int oU = 0;
-  static constexpr int oF = oU + NSLOT * NEQ * NP2;
-  static constexpr int oG = oF + NOWN * NEQ * NP2;
-  static constexpr int oFV = oG + NOWN * NEQ * NP2;
-  static constexpr int oFH = oFV + NFV * NP * 8;
+  static constexpr int oU = 0;                      // [NSLOT][ES]
+  static constexpr int oF = oU + NSLOT * ES;        // [NOWN][ES]
+  static constexpr int oG = oF + NOWN * ES;         // [NOWN][ES]
+  static constexpr int oU0 = oG + NOWN * ES;        // [NOWN][ES] u0 prefetch
+  static constexpr int oFV = oU0 + NOWN * ES;       // [NFV][NP][8]
+  static constexpr int oFH = oFV + NFV * NP * 8;    // [NFH][NP][8]
   static constexpr int oSlot = oFH + NFH * NP * 8;  // per slot: eps, Jx, Jy, dx, dy
   static constexpr int oRed = oSlot + NSLOT * 5;    // reduction scratch
   static constexpr int nDoubles = oRed + 32;
-  // ints after the doubles: element id, flags
   static constexpr int nInts = NSLOT * 2 + 8;
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
+  static_assert(2 * (bytes + 1024) <= 228 * 1024, "two CTAs must fit in one SM's shared memory");
 };
 
 constexpr int kStageThreads = 256;
@@ -76,14 +85,25 @@ constexpr int kStageThreads = 256;
 // slot flag bits
 enum : int { kSlotOwn = 1, kSlotWrap = 2, kSlotSolid = 4 };
 
+FRG_DEV void cp_async8(double* dst, const double* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+FRG_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+FRG_DEV void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 template <int NP, int FLUX, int AV>
 __global__ void __launch_bounds__(kStageThreads, 2)
     stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
   constexpr int TX = Tile2D<NP>::TX, TY = Tile2D<NP>::TY;
   using S = Smem2D<NP, TX, TY>;
-  constexpr int NEQ = 4, NP2 = NP * NP;
+  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES;
   constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, NOWN = S::NOWN;
   constexpr int NFV = S::NFV, NFH = S::NFH;
+  constexpr int NT = kStageThreads;
   constexpr bool kBR0 = (AV == kAvBR0);
   constexpr bool kAV = (AV != kAvNone);
 
@@ -91,6 +111,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   double* sU = smem + S::oU;
   double* sF = smem + S::oF;
   double* sG = smem + S::oG;
+  double* sU0 = smem + S::oU0;
   double* sFV = smem + S::oFV;
   double* sFH = smem + S::oFH;
   double* sEps = smem + S::oSlot;
@@ -101,14 +122,11 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   double* sRed = smem + S::oRed;
   int* sEl = reinterpret_cast<int*>(smem + S::nDoubles);
   int* sFlag = sEl + NSLOT;
-  int* sMisc = sFlag + NSLOT;
 
   const int tid = threadIdx.x;
-  const int nthr = blockDim.x;
   const int nx = M.nx, ny = M.ny;
   const size_t cs = (size_t)M.nel * NP2;  // component stride
 
-  // graph execution: skip finished / diverged solves
   double dt = 0.0, tstage = 0.0;
   if (B.use_sc) {
     if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
@@ -120,11 +138,12 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     dt = B.sc->dt;
   }
   const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
+  const bool need_u0 = (B.mode == kModeStage) && (B.stage != 1);
 
   const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
 
   // ---------------------------------------------------------------- slots
-  for (int s = tid; s < NSLOT; s += nthr) {
+  for (int s = tid; s < NSLOT; s += NT) {
     const int bx = s % BX, by = s / BX;
     const bool corner = (bx == 0 || bx == BX - 1) && (by == 0 || by == BY - 1);
     int gx = tx0 + bx - 1, gy = ty0 + by - 1;
@@ -160,85 +179,110 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     sEl[s] = el;
     sFlag[s] = fl;
   }
-  if (tid == 0) sMisc[0] = 0;
   __syncthreads();
 
-  // ------------------------------------------------------------- P0 load
+  // ----------------------------------------------- P0 async prefetch
   {
+    // u_s of tile + halo: rows of slots are contiguous in global memory per
+    // component, so consecutive threads copy consecutive doubles
     constexpr int ROW = BX * NP2;
-    const double* src = B.us;
-    for (int idx = tid; idx < BY * NEQ * ROW; idx += nthr) {
-      const int r = idx % ROW;
-      const int t = idx / ROW;
+    constexpr int TOTAL = BY * NEQ * ROW;
+    for (int idx = tid; idx < TOTAL; idx += NT) {
+      const int r = idx % ROW, t = idx / ROW;
       const int c = t % NEQ, by = t / NEQ;
       const int bx = r / NP2, k = r % NP2;
       const int s = by * BX + bx;
       const int el = sEl[s];
-      if (el >= 0) sU[(s * NEQ + c) * NP2 + k] = __ldg(&src[c * cs + (size_t)el * NP2 + k]);
+      if (el >= 0) cp_async8(&sU[s * ES + c * NP2 + k], &B.us[c * cs + (size_t)el * NP2 + k]);
     }
+    cp_async_commit();
+    if (need_u0) {
+      constexpr int OROW = TX * NP2;
+      constexpr int OTOTAL = TY * NEQ * OROW;
+      for (int idx = tid; idx < OTOTAL; idx += NT) {
+        const int r = idx % OROW, t = idx / OROW;
+        const int c = t % NEQ, oy = t / NEQ;
+        const int ox = r / NP2, k = r % NP2;
+        const int s = (oy + 1) * BX + ox + 1;
+        if (sFlag[s] & kSlotOwn)
+          cp_async8(&sU0[(oy * TX + ox) * ES + c * NP2 + k], &B.u0[c * cs + (size_t)sEl[s] * NP2 + k]);
+      }
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
   }
   __syncthreads();
 
   if (!prime) {
     // ------------------------------------------------------- P1 fluxes
-    for (int idx = tid; idx < NOWN * NP2; idx += nthr) {
-      const int k = idx % NP2, o = idx / NP2;
+    // item = o + NOWN*k: lanes walk over elements
+    for (int idx = tid; idx < NOWN * NP2; idx += NT) {
+      const int o = idx % NOWN, k = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn) || (sFlag[s] & kSlotSolid)) continue;
       double U[4], F[4], G[4];
 #pragma unroll
-      for (int c = 0; c < NEQ; ++c) U[c] = sU[(s * NEQ + c) * NP2 + k];
+      for (int c = 0; c < NEQ; ++c) U[c] = sU[s * ES + c * NP2 + k];
       flux_xy(P.g1, U, F, G);
+      double* fo = sF + o * ES + k;
+      double* go = sG + o * ES + k;
       if (M.curved) {
         const size_t m = (size_t)sEl[s] * NP2 + k;
         const double xxi = M.m_xxi[m], xeta = M.m_xeta[m], yxi = M.m_yxi[m], yeta = M.m_yeta[m];
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
-          sF[(o * NEQ + c) * NP2 + k] = yeta * F[c] - xeta * G[c];
-          sG[(o * NEQ + c) * NP2 + k] = -yxi * F[c] + xxi * G[c];
+          fo[c * NP2] = yeta * F[c] - xeta * G[c];
+          go[c * NP2] = -yxi * F[c] + xxi * G[c];
         }
       } else {
         const double jy = sJy[s], jx = sJx[s];
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
-          sF[(o * NEQ + c) * NP2 + k] = jy * F[c];
-          sG[(o * NEQ + c) * NP2 + k] = jx * G[c];
+          fo[c * NP2] = jy * F[c];
+          go[c * NP2] = jx * G[c];
         }
       }
     }
 
     // ------------------------------------------------------- P2 faces
-    for (int idx = tid; idx < (NFV + NFH) * NP; idx += nthr) {
+    for (int idx = tid; idx < (NFV + NFH) * NP; idx += NT) {
       const bool vert = idx < NFV * NP;
       const int id2 = vert ? idx : idx - NFV * NP;
-      const int q = id2 % NP, f = id2 / NP;
-      int sA, sB;
-      if (vert) {
-        const int fx = f % (TX + 1), fy = f / (TX + 1);
+      int f, q, sA, sB;
+      if (vert) {  // lanes walk over the faces of a row
+        const int fx = id2 % (TX + 1), r = id2 / (TX + 1);
+        q = r % NP;
+        const int fy = r / NP;
+        f = fy * (TX + 1) + fx;
         sA = (fy + 1) * BX + fx;
         sB = sA + 1;
       } else {
-        const int fx = f % TX, fy = f / TX;
+        const int fx = id2 % TX, r = id2 / TX;
+        q = r % NP;
+        const int fy = r / NP;
+        f = fy * TX + fx;
         sA = fy * BX + fx + 1;
         sB = sA + BX;
       }
       const int flA = sFlag[sA], flB = sFlag[sB];
-      double* out = (vert ? sFV : sFH) + (f * NP + q) * 8;
       if (!((flA | flB) & kSlotOwn)) continue;
+      double* out = (vert ? sFV : sFH) + (f * NP + q) * 8;
       const int eA = sEl[sA], eB = sEl[sB];
+      // the face line inside A (its east/north end) and B (west/south end)
+      const int lstride = vert ? 1 : NP;
+      const int lbase = vert ? NP * q : q;
       double uA[4], uB[4], gA[4], gB[4];
-      // traces: A's east/north face, B's west/south face
       // g traces use l^T D, whose entries sum to zero: shifting the line by
       // one of its values removes the cancellation of large terms exactly.
       if (eA >= 0) {
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
-          const double* a = sU + (sA * NEQ + c) * NP2;
-          const double vc = vert ? a[NP / 2 + NP * q] : a[q + NP * (NP / 2)];
+          const double* a = sU + sA * ES + c * NP2 + lbase;
+          const double vc = a[(NP / 2) * lstride];
           double su = 0.0, sg = 0.0;
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
-            const double v = vert ? a[i + NP * q] : a[q + NP * i];
+            const double v = a[i * lstride];
             su += ops.lR[i] * v;
             if (kBR0) sg += ops.lRD[i] * (v - vc);
           }
@@ -249,12 +293,12 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       if (eB >= 0) {
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
-          const double* b = sU + (sB * NEQ + c) * NP2;
-          const double vc = vert ? b[NP / 2 + NP * q] : b[q + NP * (NP / 2)];
+          const double* b = sU + sB * ES + c * NP2 + lbase;
+          const double vc = b[(NP / 2) * lstride];
           double su = 0.0, sg = 0.0;
 #pragma unroll
           for (int i = 0; i < NP; ++i) {
-            const double v = vert ? b[i + NP * q] : b[q + NP * i];
+            const double v = b[i * lstride];
             su += ops.lL[i] * v;
             if (kBR0) sg += ops.lLD[i] * (v - vc);
           }
@@ -375,34 +419,34 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     __syncthreads();
 
     // ------------------------------------------------ P3 xi-direction
-    for (int idx = tid; idx < NOWN * NP * NEQ; idx += nthr) {
-      const int c = idx % NEQ;
-      const int t = idx / NEQ;
-      const int j = t % NP, o = t / NP;
+    // item = o + NOWN*(j + NP*c): lanes walk over elements
+    for (int idx = tid; idx < NOWN * NP * NEQ; idx += NT) {
+      const int o = idx % NOWN, t = idx / NOWN;
+      const int j = t % NP, c = t / NP;
       const int ox = o % TX, oy = o / TX;
       const int s = (oy + 1) * BX + ox + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
-      double* Fo = sF + (o * NEQ + c) * NP2;
+      double* Fo = sF + o * ES + c * NP2 + NP * j;
       if (sFlag[s] & kSlotSolid) {
 #pragma unroll
-        for (int i = 0; i < NP; ++i) Fo[i + NP * j] = 0.0;
+        for (int i = 0; i < NP; ++i) Fo[i] = 0.0;
         continue;
       }
-      const double* Uo = sU + (s * NEQ + c) * NP2;
+      const double* Uo = sU + s * ES + c * NP2 + NP * j;
       // Dt 1 = -(gL + gR) and DtD 1 = DD 1 = 0: every line is shifted by its
       // middle value so the folded operators never cancel large terms.
       double Fl[NP], Ul[NP];
-      const double fc = Fo[NP / 2 + NP * j], uc = Uo[NP / 2 + NP * j];
+      const double fc = Fo[NP / 2], uc = Uo[NP / 2];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        Fl[k] = Fo[k + NP * j] - fc;
-        Ul[k] = Uo[k + NP * j] - uc;
+        Fl[k] = Fo[k] - fc;
+        Ul[k] = Uo[k] - uc;
       }
-      const int fW = oy * (TX + 1) + ox;
-      const double fhW = sFV[(fW * NP + j) * 8 + c] - fc;
-      const double fhE = sFV[((fW + 1) * NP + j) * 8 + c] - fc;
-      const double ghW = kBR0 ? sFV[(fW * NP + j) * 8 + 4 + c] : 0.0;
-      const double ghE = kBR0 ? sFV[((fW + 1) * NP + j) * 8 + 4 + c] : 0.0;
+      const int fWi = oy * (TX + 1) + ox;
+      const double fhW = sFV[(fWi * NP + j) * 8 + c] - fc;
+      const double fhE = sFV[((fWi + 1) * NP + j) * 8 + c] - fc;
+      const double ghW = kBR0 ? sFV[(fWi * NP + j) * 8 + 4 + c] : 0.0;
+      const double ghE = kBR0 ? sFV[((fWi + 1) * NP + j) * 8 + 4 + c] : 0.0;
       const double jx = sJx[s];
       const double rJa = M.curved ? 0.0 : 1.0 / (jx * sJy[s]);
       const double ev = kAV ? sEps[s] / (jx * jx) : 0.0;
@@ -426,39 +470,38 @@ __global__ void __launch_bounds__(kStageThreads, 2)
           for (int m = 0; m < NP; ++m) av += ops.DD[i][m] * Ul[m];
           r += ev * av;
         }
-        Fo[i + NP * j] = r;
+        Fo[i] = r;
       }
     }
     __syncthreads();
 
     // ----------------------------------------------- P4 eta-direction
-    for (int idx = tid; idx < NOWN * NP * NEQ; idx += nthr) {
-      const int c = idx % NEQ;
-      const int t = idx / NEQ;
-      const int i = t % NP, o = t / NP;
+    for (int idx = tid; idx < NOWN * NP * NEQ; idx += NT) {
+      const int o = idx % NOWN, t = idx / NOWN;
+      const int i = t % NP, c = t / NP;
       const int ox = o % TX, oy = o / TX;
       const int s = (oy + 1) * BX + ox + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
-      double* Go = sG + (o * NEQ + c) * NP2;
-      const double* Fo = sF + (o * NEQ + c) * NP2;
+      double* Go = sG + o * ES + c * NP2 + i;
+      const double* Fo = sF + o * ES + c * NP2 + i;
       if (sFlag[s] & kSlotSolid) {
 #pragma unroll
-        for (int j = 0; j < NP; ++j) Go[i + NP * j] = 0.0;
+        for (int j = 0; j < NP; ++j) Go[NP * j] = 0.0;
         continue;
       }
-      const double* Uo = sU + (s * NEQ + c) * NP2;
+      const double* Uo = sU + s * ES + c * NP2 + i;
       double Gl[NP], Ul[NP];
-      const double gc = Go[i + NP * (NP / 2)], uc = Uo[i + NP * (NP / 2)];
+      const double gc = Go[NP * (NP / 2)], uc = Uo[NP * (NP / 2)];
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
-        Gl[k] = Go[i + NP * k] - gc;
-        Ul[k] = Uo[i + NP * k] - uc;
+        Gl[k] = Go[NP * k] - gc;
+        Ul[k] = Uo[NP * k] - uc;
       }
-      const int fS = oy * TX + ox;
-      const double fhS = sFH[(fS * NP + i) * 8 + c] - gc;
-      const double fhN = sFH[((fS + TX) * NP + i) * 8 + c] - gc;
-      const double ghS = kBR0 ? sFH[(fS * NP + i) * 8 + 4 + c] : 0.0;
-      const double ghN = kBR0 ? sFH[((fS + TX) * NP + i) * 8 + 4 + c] : 0.0;
+      const int fSi = oy * TX + ox;
+      const double fhS = sFH[(fSi * NP + i) * 8 + c] - gc;
+      const double fhN = sFH[((fSi + TX) * NP + i) * 8 + c] - gc;
+      const double ghS = kBR0 ? sFH[(fSi * NP + i) * 8 + 4 + c] : 0.0;
+      const double ghN = kBR0 ? sFH[((fSi + TX) * NP + i) * 8 + 4 + c] : 0.0;
       const double jy = sJy[s];
       const double rJa = M.curved ? 0.0 : 1.0 / (sJx[s] * jy);
       const double ev = kAV ? sEps[s] / (jy * jy) : 0.0;
@@ -470,7 +513,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Gl[k];
         const double rJ = M.curved ? M.m_rJ[mbase + NP * j] : rJa;
-        double r = Fo[i + NP * j] - acc * rJ;
+        double r = Fo[NP * j] - acc * rJ;
         if (kBR0) {
           double av = 0.0;
 #pragma unroll
@@ -482,54 +525,56 @@ __global__ void __launch_bounds__(kStageThreads, 2)
           for (int m = 0; m < NP; ++m) av += ops.DD[j][m] * Ul[m];
           r += ev * av;
         }
-        Go[i + NP * j] = r;
+        Go[NP * j] = r;
       }
     }
+    cp_async_wait<0>();  // u0 prefetch has landed
     __syncthreads();
 
     // --------------------------------------------------- P5 epilogue
     {
-      constexpr int ROW = TX * NP2;
+      constexpr int OROW = TX * NP2;
       int bad_du = 0, bad_u = 0;
       const double cdt = B.c * dt;
-      for (int idx = tid; idx < TY * NEQ * ROW; idx += nthr) {
-        const int r = idx % ROW;
-        const int t = idx / ROW;
+      for (int idx = tid; idx < TY * NEQ * OROW; idx += NT) {
+        const int r = idx % OROW, t = idx / OROW;
         const int c = t % NEQ, oy = t / NEQ;
         const int ox = r / NP2, k = r % NP2;
         const int o = oy * TX + ox;
         const int s = (oy + 1) * BX + ox + 1;
         if (!(sFlag[s] & kSlotOwn)) continue;
-        const double du = sG[(o * NEQ + c) * NP2 + k];
+        const int li = o * ES + c * NP2 + k;
+        const double du = sG[li];
         const size_t gi = c * cs + (size_t)sEl[s] * NP2 + k;
         if (B.mode == kModeResidual) {
           B.du_out[gi] = du;
           bad_du |= !isfinite(du);
           continue;
         }
-        const double us = sU[(s * NEQ + c) * NP2 + k];
-        const double u0 = (B.stage == 1) ? us : B.u0[gi];
+        const double us = sU[s * ES + c * NP2 + k];
+        const double u0 = (B.stage == 1) ? us : sU0[li];
         const double un = (B.a * u0 + B.b * us) + cdt * du;
         B.uout[gi] = un;
-        sF[(o * NEQ + c) * NP2 + k] = un;
+        sF[li] = un;
         bad_du |= !isfinite(du);
         bad_u |= !isfinite(un);
       }
       const int any_du = __syncthreads_or(bad_du);
       const int any_u = __syncthreads_or(bad_u);
       if (tid == 0 && (any_du || any_u)) {
-        if (B.sc) atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
+        if (B.sc)
+          atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
       }
     }
     if (B.mode == kModeResidual) return;
   } else {
+    cp_async_wait<0>();
+    __syncthreads();
     // prime / sense: the "new" state is the loaded state
-    for (int idx = tid; idx < NOWN * NEQ * NP2; idx += nthr) {
-      const int k = idx % NP2;
-      const int t = idx / NP2;
-      const int c = t % NEQ, o = t / NEQ;
+    for (int idx = tid; idx < NOWN * NEQ * NP2; idx += NT) {
+      const int o = idx % NOWN, r = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (sFlag[s] & kSlotOwn) sF[(o * NEQ + c) * NP2 + k] = sU[(s * NEQ + c) * NP2 + k];
+      if (sFlag[s] & kSlotOwn) sF[o * ES + r] = sU[s * ES + r];
     }
     __syncthreads();
   }
@@ -537,37 +582,38 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   // ------------------------------------------ P6 sensor / eps / lambda
   if (!(kAV || B.want_lambda || B.mode == kModeSense)) return;
   {
-    double* sWS = sG;             // [NOWN][NP2] wave speeds
-    double* sX = sG + NOWN * NP2;  // [NOWN][NP2] V^{-1} rho
-    double* sPart = sX + NOWN * NP2;  // [NOWN][NP][2]
+    constexpr int WS = odd_up(NP2);
+    double* sWS = sG;                // [NOWN][WS] wave speeds
+    double* sX = sG + NOWN * WS;     // [NOWN][WS] V^{-1} rho
+    double* sPart = sX + NOWN * WS;  // [NOWN*NP][2]
     double lmax = 0.0;
-    for (int idx = tid; idx < NOWN * NP2; idx += nthr) {
-      const int k = idx % NP2, o = idx / NP2;
+    for (int idx = tid; idx < NOWN * NP2; idx += NT) {
+      const int o = idx % NOWN, k = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
       double U[4];
 #pragma unroll
-      for (int c = 0; c < NEQ; ++c) U[c] = sF[(o * NEQ + c) * NP2 + k];
+      for (int c = 0; c < NEQ; ++c) U[c] = sF[o * ES + c * NP2 + k];
       const double w = wave_speed2(P.gamma, P.g1, U);
-      sWS[o * NP2 + k] = w;
+      sWS[o * WS + k] = w;
       lmax = jmax(lmax, w);
     }
     if (kAV || B.mode == kModeSense) {
       // X = V^{-1} rho, column by column
-      for (int idx = tid; idx < NOWN * NP; idx += nthr) {
-        const int j = idx % NP, o = idx / NP;
+      for (int idx = tid; idx < NOWN * NP; idx += NT) {
+        const int o = idx % NOWN, j = idx / NOWN;
         const int s = (o / TX + 1) * BX + (o % TX) + 1;
         if (!(sFlag[s] & kSlotOwn)) continue;
-        const double* rho = sF + (o * NEQ) * NP2;
+        const double* rho = sF + o * ES + NP * j;
         double col[NP];
 #pragma unroll
-        for (int k = 0; k < NP; ++k) col[k] = rho[k + NP * j];
+        for (int k = 0; k < NP; ++k) col[k] = rho[k];
 #pragma unroll
         for (int i = 0; i < NP; ++i) {
           double a = 0.0;
 #pragma unroll
           for (int k = 0; k < NP; ++k) a += ops.Vinv[i][k] * col[k];
-          sX[o * NP2 + i + NP * j] = a;
+          sX[o * WS + i + NP * j] = a;
         }
       }
     }
@@ -578,19 +624,19 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     }
     __syncthreads();
     if (B.want_lambda && tid < 32) {
-      double v = (tid < (nthr >> 5)) ? sRed[tid] : 0.0;
+      double v = (tid < (NT >> 5)) ? sRed[tid] : 0.0;
       for (int off = 16; off > 0; off >>= 1) v = jmax(v, __shfl_xor_sync(0xffffffffu, v, off));
       if (tid == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, v);
     }
     if (!(kAV || B.mode == kModeSense)) return;
     // Uhat = X V^{-T}: row i energies
-    for (int idx = tid; idx < NOWN * NP; idx += nthr) {
-      const int i = idx % NP, o = idx / NP;
+    for (int idx = tid; idx < NOWN * NP; idx += NT) {
+      const int o = idx % NOWN, i = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
       double row[NP];
 #pragma unroll
-      for (int k = 0; k < NP; ++k) row[k] = sX[o * NP2 + i + NP * k];
+      for (int k = 0; k < NP; ++k) row[k] = sX[o * WS + i + NP * k];
       double etot = 0.0, ehigh = 0.0;
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
@@ -605,7 +651,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       sPart[(o * NP + i) * 2 + 1] = ehigh;
     }
     __syncthreads();
-    for (int o = tid; o < NOWN; o += nthr) {
+    for (int o = tid; o < NOWN; o += NT) {
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
       const int el = sEl[s];
@@ -616,7 +662,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         ehigh += sPart[(o * NP + i) * 2 + 1];
       }
 #pragma unroll
-      for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * NP2 + k]);
+      for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * WS + k]);
       lam = jmax(lam, kEps);
       const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
       if (B.mode == kModeSense) {
