@@ -197,8 +197,9 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    # warm-up (untimed)
+    # warm-up (untimed): autotune the stage-kernel tile variant, then steps
     solve.upload(u_host.numpy().reshape(st.u.shape, order="F"), 0.0)
+    variant, variant_ms = solve.autotune(reps=5)
     r = solve.advance(1e9, cfl=C3.cfl, max_steps=max(3, args.warmup))
     if r["status"] == "diverged":
         raise RuntimeError("warm-up diverged")
@@ -273,7 +274,9 @@ def run_ours(args):
                          "frac": achieved_gbs / peak, "traffic": tr,
                          "kernel": "frg::stage2d_kernel<4,HLLC,BR0>",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "stage_ms": [float(x) for x in stage_ms], "peak_kind": peak_kind},
+                         "stage_ms": [float(x) for x in stage_ms], "peak_kind": peak_kind,
+                         "tile_variant": int(variant),
+                         "variant_ms": [float(x) for x in variant_ms]},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": args.steps * 5,

@@ -105,6 +105,9 @@ SIGNATURES = {
                               C.POINTER(frg_result)]),
     "frg_time_stages": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, _dp,
                                   C.POINTER(frg_result)]),
+    "frg_get_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "frg_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "frg_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp]),
 }
 
 _lib = None

@@ -28,6 +28,22 @@ int launch_stage1d_np3(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np4(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np5(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np6(const Launch1D&, const StageBufs&, cudaStream_t);
+int stage2d_variants_np2();
+int stage2d_variants_np3();
+int stage2d_variants_np4();
+int stage2d_variants_np5();
+int stage2d_variants_np6();
+
+int stage2d_variants(int np) {
+  switch (np) {
+    case 2: return stage2d_variants_np2();
+    case 3: return stage2d_variants_np3();
+    case 4: return stage2d_variants_np4();
+    case 5: return stage2d_variants_np5();
+    case 6: return stage2d_variants_np6();
+  }
+  return 1;
+}
 
 int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
@@ -661,6 +677,7 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
     s->L2.phys = P;
     s->L2.flux = d->flux;
     s->L2.av = av;
+    s->L2.variant = 0;
     s->L1.ops = &s->ops;
     s->L1.phys = P;
     s->L1.flux = d->flux;
@@ -900,6 +917,79 @@ int frg_time_stages(frg_solve* s, int64_t nsteps, double cfl, double fixed_dt, d
   if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
   if (nsteps < 1) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "nsteps must be >= 1");
   return run_steps(s, INFINITY, cfl, fixed_dt, nsteps, out, false, stage_ms);
+}
+
+int frg_get_variant(const frg_solve* s, int* variant, int* n_variants) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  if (variant) *variant = s->dim == 2 ? s->L2.variant : 0;
+  if (n_variants) *n_variants = s->dim == 2 ? stage2d_variants(s->np) : 1;
+  return FRG_OK;
+}
+
+int frg_set_variant(frg_solve* s, int variant) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  const int n = s->dim == 2 ? stage2d_variants(s->np) : 1;
+  if (variant < 0 || variant >= n) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "variant out of range");
+  if (s->dim == 2 && s->L2.variant != variant) {
+    s->L2.variant = variant;
+    if (s->graph) {  // graphs bake the launch configuration
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+  }
+  return FRG_OK;
+}
+
+int frg_autotune(frg_solve* s, int reps, int* best, double* ms) {
+  if (!s || reps < 1) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  cudaSetDevice(s->ctx->device);
+  int rc = make_current_canonical(s);
+  if (rc) return rc;
+  const int n = s->dim == 2 ? stage2d_variants(s->np) : 1;
+  const int saved = s->dim == 2 ? s->L2.variant : 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best_ms = INFINITY;
+  int best_v = 0;
+  for (int v = 0; v < n; ++v) {
+    if (s->dim == 2) s->L2.variant = v;
+    if ((rc = prime(s, 0, false))) break;
+    // a stage-2 style launch that writes only scratch buffers
+    StageBufs b{};
+    b.us = s->U[0];
+    b.u0 = s->U[0];
+    b.uout = s->U[2];
+    b.eps_in = s->E[0];
+    b.eps_out = s->E[2];
+    b.a = 3.0 / 4.0;
+    b.b = 1.0 / 4.0;
+    b.c = 1.0 / 4.0;
+    b.stage = 2;
+    b.mode = kModeStage;
+    b.want_lambda = 1;
+    if ((rc = launch(s, b))) break;  // warm-up (function attributes, caches)
+    cudaEventRecord(e0, s->ctx->stream);
+    for (int r = 0; r < reps && !rc; ++r) rc = launch(s, b);
+    cudaEventRecord(e1, s->ctx->stream);
+    if (rc) break;
+    if ((rc = cuda_err(s->ctx, cudaEventSynchronize(e1), "autotune"))) break;
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    const double per = (double)t / reps;
+    if (ms) ms[v] = per;
+    if (per < best_ms) {
+      best_ms = per;
+      best_v = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s->dim == 2) s->L2.variant = saved;
+  if (rc) return rc;
+  if (best) *best = best_v;
+  return frg_set_variant(s, best_v);
 }
 
 int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps, frg_result* out) {

@@ -149,8 +149,9 @@ struct Launch2D {
   const HostOps* ops;
   Mesh2Dev mesh;
   Phys phys;
-  int flux;  // FRG_FLUX_*
-  int av;    // kAv*
+  int flux;     // FRG_FLUX_*
+  int av;       // kAv*
+  int variant;  // tile variant (autotuned)
 };
 struct Launch1D {
   const HostOps* ops;
@@ -162,6 +163,6 @@ struct Launch1D {
 // Returns 0 or a CUDA error code.
 int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream);
 int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream);
-int stage2d_smem_bytes(int np, int av);
+int stage2d_variants(int np);
 
 }  // namespace frg

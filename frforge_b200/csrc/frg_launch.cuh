@@ -31,20 +31,78 @@ OpsT<NP> make_ops(const HostOps& h) {
   return o;
 }
 
-template <int NP, int FLUX, int AV>
-int launch2d_inst(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
-  using T = Tile2D<NP>;
-  using S = Smem2D<NP, T::TX, T::TY>;
-  auto kern = stage2d_kernel<NP, FLUX, AV>;
-  static bool configured = false;  // per instance; attribute is per function
+// Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory).
+// Variant 0 is the default; the autotuner times all of them on the solve.
+template <int NP>
+struct Variants2D;
+template <>
+struct Variants2D<2> {
+  static constexpr int n = 2;
+  template <int V> struct V_;
+};
+template <> template <> struct Variants2D<2>::V_<0> { static constexpr int TX = 8, TY = 8, MINB = 2; static constexpr bool U0S = true; };
+template <> template <> struct Variants2D<2>::V_<1> { static constexpr int TX = 8, TY = 4, MINB = 3; static constexpr bool U0S = false; };
+template <>
+struct Variants2D<3> {
+  static constexpr int n = 3;
+  template <int V> struct V_;
+};
+template <> template <> struct Variants2D<3>::V_<0> { static constexpr int TX = 8, TY = 6, MINB = 2; static constexpr bool U0S = true; };
+template <> template <> struct Variants2D<3>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> template <> struct Variants2D<3>::V_<2> { static constexpr int TX = 4, TY = 4, MINB = 4; static constexpr bool U0S = false; };
+template <>
+struct Variants2D<4> {
+  static constexpr int n = 3;
+  template <int V> struct V_;
+};
+template <> template <> struct Variants2D<4>::V_<0> { static constexpr int TX = 8, TY = 4, MINB = 2; static constexpr bool U0S = true; };
+template <> template <> struct Variants2D<4>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> template <> struct Variants2D<4>::V_<2> { static constexpr int TX = 8, TY = 2, MINB = 4; static constexpr bool U0S = false; };
+template <>
+struct Variants2D<5> {
+  static constexpr int n = 2;
+  template <int V> struct V_;
+};
+template <> template <> struct Variants2D<5>::V_<0> { static constexpr int TX = 4, TY = 4, MINB = 2; static constexpr bool U0S = true; };
+template <> template <> struct Variants2D<5>::V_<1> { static constexpr int TX = 4, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <>
+struct Variants2D<6> {
+  static constexpr int n = 2;
+  template <int V> struct V_;
+};
+template <> template <> struct Variants2D<6>::V_<0> { static constexpr int TX = 4, TY = 3, MINB = 2; static constexpr bool U0S = true; };
+template <> template <> struct Variants2D<6>::V_<1> { static constexpr int TX = 3, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+
+template <int NP, int FLUX, int AV, int V>
+int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
+  using VV = typename Variants2D<NP>::template V_<V>;
+  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB>;
+  auto kern = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S>;
+  static bool configured = false;  // the attribute belongs to the function
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
     if (e != cudaSuccess) return (int)e;
     configured = true;
   }
-  dim3 grid((L.mesh.nx + T::TX - 1) / T::TX, (L.mesh.ny + T::TY - 1) / T::TY);
+  dim3 grid((L.mesh.nx + VV::TX - 1) / VV::TX, (L.mesh.ny + VV::TY - 1) / VV::TY);
   kern<<<grid, kStageThreads, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
   return (int)cudaGetLastError();
+}
+
+template <int NP, int FLUX, int AV>
+int launch2d_inst(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
+  const int v = (L.variant >= 0 && L.variant < Variants2D<NP>::n) ? L.variant : 0;
+  switch (v) {
+    case 1:
+      if constexpr (Variants2D<NP>::n > 1) return launch2d_var<NP, FLUX, AV, 1>(L, b, st);
+      break;
+    case 2:
+      if constexpr (Variants2D<NP>::n > 2) return launch2d_var<NP, FLUX, AV, 2>(L, b, st);
+      break;
+    default:
+      break;
+  }
+  return launch2d_var<NP, FLUX, AV, 0>(L, b, st);
 }
 
 template <int NP, int FLUX, int AV>
@@ -95,9 +153,8 @@ int launch1d_np(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
 }
 
 template <int NP>
-size_t smem2d_bytes() {
-  using T = Tile2D<NP>;
-  return Smem2D<NP, T::TX, T::TY>::bytes;
+int variants2d() {
+  return Variants2D<NP>::n;
 }
 
 }  // namespace frg
@@ -110,5 +167,5 @@ size_t smem2d_bytes() {
   int launch_stage1d_np##NPV(const Launch1D& L, const StageBufs& b, cudaStream_t st) {       \
     return launch1d_np<NPV>(L, b, st);                                                       \
   }                                                                                          \
-  size_t stage2d_smem_np##NPV() { return smem2d_bytes<NPV>(); }                              \
+  int stage2d_variants_np##NPV() { return variants2d<NPV>(); }                                \
   }

@@ -59,25 +59,28 @@ struct Tile2D<6> {
 
 constexpr int odd_up(int n) { return (n % 2) ? n : n + 1; }
 
-template <int NP, int TX, int TY>
+// U0S: stage the step-start state u0 in shared memory (prefetched under the
+// compute); otherwise the epilogue reads it from global memory.
+template <int NP, int TX, int TY, bool U0S = true, int MINB = 2>
 struct Smem2D {
   static constexpr int NEQ = 4, NP2 = NP * NP;
   static constexpr int BX = TX + 2, BY = TY + 2, NSLOT = BX * BY, NOWN = TX * TY;
   static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
   static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
+  static constexpr int FS = odd_up(NP * 8);     // face stride: NP points x (fhat[4], ghat[4])
   // doubles
   static constexpr int oU = 0;                      // [NSLOT][ES]
   static constexpr int oF = oU + NSLOT * ES;        // [NOWN][ES]
   static constexpr int oG = oF + NOWN * ES;         // [NOWN][ES]
   static constexpr int oU0 = oG + NOWN * ES;        // [NOWN][ES] u0 prefetch
-  static constexpr int oFV = oU0 + NOWN * ES;       // [NFV][NP][8]
-  static constexpr int oFH = oFV + NFV * NP * 8;    // [NFH][NP][8]
-  static constexpr int oSlot = oFH + NFH * NP * 8;  // per slot: eps, Jx, Jy, dx, dy
+  static constexpr int oFV = oU0 + (U0S ? NOWN * ES : 0);  // [NFV][FS]
+  static constexpr int oFH = oFV + NFV * FS;        // [NFH][FS]
+  static constexpr int oSlot = oFH + NFH * FS;      // per slot: eps, Jx, Jy, dx, dy
   static constexpr int oRed = oSlot + NSLOT * 5;    // reduction scratch
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2 + 8;
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
-  static_assert(2 * (bytes + 1024) <= 228 * 1024, "two CTAs must fit in one SM's shared memory");
+  static_assert(MINB * (bytes + 1024) <= 228 * 1024, "MINB CTAs must fit in one SM's shared memory");
 };
 
 constexpr int kStageThreads = 256;
@@ -95,12 +98,14 @@ FRG_DEV void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-template <int NP, int FLUX, int AV>
-__global__ void __launch_bounds__(kStageThreads, 2)
+// TX x TY: tile (elements); MINB: CTAs per SM the register budget targets;
+// U0S: u0 staged in shared memory.
+template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
+          bool U0S = true>
+__global__ void __launch_bounds__(kStageThreads, MINB)
     stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
-  constexpr int TX = Tile2D<NP>::TX, TY = Tile2D<NP>::TY;
-  using S = Smem2D<NP, TX, TY>;
-  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES;
+  using S = Smem2D<NP, TX, TY, U0S, MINB>;
+  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
   constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, NOWN = S::NOWN;
   constexpr int NFV = S::NFV, NFH = S::NFH;
   constexpr int NT = kStageThreads;
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       if (el >= 0) cp_async8(&sU[s * ES + c * NP2 + k], &B.us[c * cs + (size_t)el * NP2 + k]);
     }
     cp_async_commit();
-    if (need_u0) {
+    if (U0S && need_u0) {
       constexpr int OROW = TX * NP2;
       constexpr int OTOTAL = TY * NEQ * OROW;
       for (int idx = tid; idx < OTOTAL; idx += NT) {
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       }
       const int flA = sFlag[sA], flB = sFlag[sB];
       if (!((flA | flB) & kSlotOwn)) continue;
-      double* out = (vert ? sFV : sFH) + (f * NP + q) * 8;
+      double* out = (vert ? sFV : sFH) + f * FS + q * 8;
       const int eA = sEl[sA], eB = sEl[sB];
       // the face line inside A (its east/north end) and B (west/south end)
       const int lstride = vert ? 1 : NP;
@@ -443,10 +448,11 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         Ul[k] = Uo[k] - uc;
       }
       const int fWi = oy * (TX + 1) + ox;
-      const double fhW = sFV[(fWi * NP + j) * 8 + c] - fc;
-      const double fhE = sFV[((fWi + 1) * NP + j) * 8 + c] - fc;
-      const double ghW = kBR0 ? sFV[(fWi * NP + j) * 8 + 4 + c] : 0.0;
-      const double ghE = kBR0 ? sFV[((fWi + 1) * NP + j) * 8 + 4 + c] : 0.0;
+      const double* fw = sFV + fWi * FS + j * 8 + c;
+      const double fhW = fw[0] - fc;
+      const double fhE = fw[FS] - fc;
+      const double ghW = kBR0 ? fw[4] : 0.0;
+      const double ghE = kBR0 ? fw[FS + 4] : 0.0;
       const double jx = sJx[s];
       const double rJa = M.curved ? 0.0 : 1.0 / (jx * sJy[s]);
       const double ev = kAV ? sEps[s] / (jx * jx) : 0.0;
@@ -498,10 +504,11 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         Ul[k] = Uo[NP * k] - uc;
       }
       const int fSi = oy * TX + ox;
-      const double fhS = sFH[(fSi * NP + i) * 8 + c] - gc;
-      const double fhN = sFH[((fSi + TX) * NP + i) * 8 + c] - gc;
-      const double ghS = kBR0 ? sFH[(fSi * NP + i) * 8 + 4 + c] : 0.0;
-      const double ghN = kBR0 ? sFH[((fSi + TX) * NP + i) * 8 + 4 + c] : 0.0;
+      const double* fs = sFH + fSi * FS + i * 8 + c;
+      const double fhS = fs[0] - gc;
+      const double fhN = fs[TX * FS] - gc;
+      const double ghS = kBR0 ? fs[4] : 0.0;
+      const double ghN = kBR0 ? fs[TX * FS + 4] : 0.0;
       const double jy = sJy[s];
       const double rJa = M.curved ? 0.0 : 1.0 / (sJx[s] * jy);
       const double ev = kAV ? sEps[s] / (jy * jy) : 0.0;
@@ -552,7 +559,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
           continue;
         }
         const double us = sU[s * ES + c * NP2 + k];
-        const double u0 = (B.stage == 1) ? us : sU0[li];
+        const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : __ldg(&B.u0[gi]));
         const double un = (B.a * u0 + B.b * us) + cdt * du;
         B.uout[gi] = un;
         sF[li] = un;
@@ -582,10 +589,10 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   // ------------------------------------------ P6 sensor / eps / lambda
   if (!(kAV || B.want_lambda || B.mode == kModeSense)) return;
   {
-    constexpr int WS = odd_up(NP2);
+    constexpr int WS = odd_up(NP2), PS = odd_up(2 * NP);
     double* sWS = sG;                // [NOWN][WS] wave speeds
     double* sX = sG + NOWN * WS;     // [NOWN][WS] V^{-1} rho
-    double* sPart = sX + NOWN * WS;  // [NOWN*NP][2]
+    double* sPart = sX + NOWN * WS;  // [NOWN][PS] row energies
     double lmax = 0.0;
     for (int idx = tid; idx < NOWN * NP2; idx += NT) {
       const int o = idx % NOWN, k = idx / NOWN;
@@ -647,8 +654,8 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         etot += a2;
         if (i == NP - 1 || j == NP - 1) ehigh += a2;
       }
-      sPart[(o * NP + i) * 2 + 0] = etot;
-      sPart[(o * NP + i) * 2 + 1] = ehigh;
+      sPart[o * PS + 2 * i + 0] = etot;
+      sPart[o * PS + 2 * i + 1] = ehigh;
     }
     __syncthreads();
     for (int o = tid; o < NOWN; o += NT) {
@@ -658,8 +665,8 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       double etot = 0.0, ehigh = 0.0, lam = 0.0;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
-        etot += sPart[(o * NP + i) * 2 + 0];
-        ehigh += sPart[(o * NP + i) * 2 + 1];
+        etot += sPart[o * PS + 2 * i + 0];
+        ehigh += sPart[o * PS + 2 * i + 1];
       }
 #pragma unroll
       for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * WS + k]);

@@ -225,6 +225,24 @@ class GpuSolve:
                   "frg_advance")
         return {"status": L.STATUS_SYMBOL[r.status], "n_steps": int(r.n_steps), "t": r.t}
 
+    def variant(self):
+        """(current tile variant, number of variants) of the stage kernel."""
+        v, n = C.c_int(), C.c_int()
+        self._chk(L.load().frg_get_variant(self.handle, C.byref(v), C.byref(n)), "frg_get_variant")
+        return v.value, n.value
+
+    def set_variant(self, v: int) -> None:
+        self._chk(L.load().frg_set_variant(self.handle, int(v)), "frg_set_variant")
+
+    def autotune(self, reps: int = 5):
+        """Time every tile variant on the current state and keep the fastest;
+        returns (best, per-variant ms)."""
+        _, n = self.variant()
+        ms = np.zeros(max(n, 1))
+        best = C.c_int()
+        self._chk(L.load().frg_autotune(self.handle, int(reps), C.byref(best), L.dptr(ms)), "frg_autotune")
+        return best.value, ms[:n]
+
     def time_stages(self, nsteps: int, cfl: float = 0.2, dt: Optional[float] = None):
         """Run nsteps steps with every stage kernel bracketed by CUDA events;
         returns (mean stage-kernel ms per stage, result dict)."""

@@ -200,6 +200,15 @@ int frg_step(frg_solve* s, double dt, int* step_status);
 int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt,
                 int64_t max_steps, frg_result* out);
 
+/* Stage-kernel tile variants (elements per CTA, CTAs per SM, u0 staging),
+   no reference counterpart.  frg_autotune times every variant on the
+   solve's current state (scratch buffers only; the state is untouched) with
+   `reps` launches each, selects the fastest and returns it in *best; ms (may
+   be NULL) receives the mean launch time of each variant. */
+int frg_get_variant(const frg_solve* s, int* variant, int* n_variants);
+int frg_set_variant(frg_solve* s, int variant);
+int frg_autotune(frg_solve* s, int reps, int* best, double* ms);
+
 /* Instrumented frg_advance for profiling (no reference counterpart): runs
    nsteps steps with direct launches and times every stage kernel with CUDA
    events on the solve's stream; stage_ms[k] = mean duration (ms) of the

@@ -47,21 +47,25 @@ CASES_2D = [
 @pytest.mark.parametrize("cfg", CASES_2D, ids=lambda c: "-".join(f"{k}={v}" for k, v in c.items() if k != "bcs"))
 @pytest.mark.parametrize("ic", ["smooth", "shock"])
 def test_residual_2d(cfg, ic):
-    # identical inputs: the reference's operator tables go through the ABI
-    orc, state, solve = pair_2d(caller_ops=True, **cfg)
+    # identical inputs: the reference's operator tables and its (D-differentiated)
+    # metric arrays go through the ABI
+    orc, state, solve = pair_2d(caller_ops=True, gpu_metrics=True, **cfg)
     u = smooth_state_2d(orc) if ic == "smooth" else four_quadrant_state(orc)
     got, ref = _residual_pair(orc, state, solve, u)
     assert np.all(np.isfinite(got))
     assert rel_linf(got, ref) <= RES_TOL, rel_linf(got, ref)
 
 
-@pytest.mark.parametrize("p", [2, 3, 4, 5])
-def test_residual_2d_library_tables(p):
-    # the library's own build_operators (Newton GL nodes) differs from the
-    # reference's eigen-based tables by ~1 ulp in the nodes; residuals then
-    # agree to a few 1e-13 of max|du|
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("ic", ["smooth", "shock"])
+def test_residual_2d_affine_path(p, ic):
+    # the production path: library-built tables (Newton GL nodes, ~1 ulp from
+    # the reference's eigen-based nodes) and exact affine metrics (the
+    # reference differentiates x(xi) with D, which leaves ~1e-14 relative
+    # error in x_xi, y_eta at P=5); agreement is then a few 1e-12 of max|du|
     orc, state, solve = pair_2d(p=p, method="persson", flux="hllc", bcs=("transmissive",) * 4)
-    got, ref = _residual_pair(orc, state, solve, four_quadrant_state(orc))
+    u = smooth_state_2d(orc) if ic == "smooth" else four_quadrant_state(orc)
+    got, ref = _residual_pair(orc, state, solve, u)
     assert rel_linf(got, ref) <= 1e-11
 
 
@@ -90,7 +94,8 @@ def test_residual_2d_solid_mask():
     for jy in range(2):
         for jx in range(4, nx):
             solid[jy * nx + jx] = True
-    orc, state, solve = pair_2d(p=2, nx=nx, ny=ny, method="persson", flux="hllc", solid=solid, caller_ops=True,
+    orc, state, solve = pair_2d(p=2, nx=nx, ny=ny, method="persson", flux="hllc", solid=solid,
+                                caller_ops=True, gpu_metrics=True,
                                 bcs=(("dirichlet", (1.4, 4.2, 0.0, 2.5 + 0.5 * 1.4 * 9)), "transmissive",
                                      "reflecting", "reflecting"))
     u = smooth_state_2d(orc)
@@ -98,6 +103,26 @@ def test_residual_2d_solid_mask():
     assert rel_linf(got, ref) <= RES_TOL
     blk = got.reshape(-1, nx * ny, 4, order="F")
     assert np.all(blk[:, solid, :] == 0.0)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+def test_tile_variants_agree(p):
+    # every tile variant of the stage kernel is a separate instantiation
+    orc, state, solve = pair_2d(p=p, nx=11, ny=9, method="persson", flux="hllc", caller_ops=True,
+                                gpu_metrics=True, bcs=("transmissive",) * 4)
+    u = four_quadrant_state(orc)
+    orc.set_state(u)
+    ref = orc.residual()
+    _, n = solve.variant()
+    assert n >= 2
+    for v in range(n):
+        solve.set_variant(v)
+        solve.upload(u, 0.0)
+        assert rel_linf(solve.residual(), ref) <= RES_TOL, v
+    solve.upload(u, 0.0)
+    best, ms = solve.autotune(reps=2)
+    assert 0 <= best < n and np.all(ms > 0)
+    assert solve.variant()[0] == best
 
 
 def test_freestream_residual_2d():
