@@ -18,6 +18,11 @@ namespace frg {
 
 #define FRG_DEV __device__ __forceinline__
 
+// Floor max(x, c) for a finite constant c with Julia's NaN propagation:
+// fmax drops a NaN operand, and adding x - x (0 for finite x, NaN otherwise)
+// puts it back.
+FRG_DEV double jfloor(double x, double c) { return fmax(x, c) + (x - x); }
+
 // NaN-propagating max/min (Julia semantics for Float64).
 FRG_DEV double jmax(double a, double b) {
   double r = fmax(a, b);
@@ -32,7 +37,7 @@ FRG_DEV double jmin(double a, double b) {
 
 // Physical fluxes F(U), G(U): physical_flux_x!/y!, Euler2D.jl:54-79.
 FRG_DEV void flux_xy(double g1, const double U[4], double F[4], double G[4]) {
-  const double r = jmax(U[0], kEps);
+  const double r = jfloor(U[0], kEps);
   const double ri = 1.0 / r;
   const double u = U[1] * ri, v = U[2] * ri;
   const double p = g1 * (U[3] - 0.5 * r * (u * u + v * v));
@@ -48,10 +53,10 @@ FRG_DEV void flux_xy(double g1, const double U[4], double F[4], double G[4]) {
 
 // max(|u|+c, |v|+c) at one state: max_wave_speed, Euler2D.jl:92-105.
 FRG_DEV double wave_speed2(double gamma, double g1, const double U[4]) {
-  const double r = jmax(U[0], kEps);
+  const double r = jfloor(U[0], kEps);
   const double ri = 1.0 / r;
   const double u = U[1] * ri, v = U[2] * ri;
-  const double p = jmax(g1 * (U[3] - 0.5 * r * (u * u + v * v)), kEps);
+  const double p = jfloor(g1 * (U[3] - 0.5 * r * (u * u + v * v)), kEps);
   const double c = sqrt(gamma * p * ri);
   return jmax(fabs(u) + c, fabs(v) + c);
 }
@@ -59,10 +64,10 @@ FRG_DEV double wave_speed2(double gamma, double g1, const double U[4]) {
 // Rusanov normal flux, numerical_flux_n!, Euler2D.jl:114-150.
 FRG_DEV void rusanov2(double gamma, double g1, const double uL[4], const double uR[4],
                       double nx, double ny, double out[4]) {
-  const double rL = jmax(uL[0], kEps), riL = 1.0 / rL;
+  const double rL = jfloor(uL[0], kEps), riL = 1.0 / rL;
   const double uLv = uL[1] * riL, vLv = uL[2] * riL;
   const double pL = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
-  const double rR = jmax(uR[0], kEps), riR = 1.0 / rR;
+  const double rR = jfloor(uR[0], kEps), riR = 1.0 / rR;
   const double uRv = uR[1] * riR, vRv = uR[2] * riR;
   const double pR = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
   const double unL = uLv * nx + vLv * ny, unR = uRv * nx + vRv * ny;
@@ -74,8 +79,8 @@ FRG_DEV void rusanov2(double gamma, double g1, const double uL[4], const double 
   const double fR1 = (uR[1] * uRv + pR) * nx + (uR[1] * vRv) * ny;
   const double fR2 = (uR[2] * uRv) * nx + (uR[2] * vRv + pR) * ny;
   const double fR3 = (uR[3] + pR) * unR;
-  const double cL = sqrt(gamma * jmax(pL, kEps) * riL);
-  const double cR = sqrt(gamma * jmax(pR, kEps) * riR);
+  const double cL = sqrt(gamma * jfloor(pL, kEps) * riL);
+  const double cR = sqrt(gamma * jfloor(pR, kEps) * riR);
   const double lam = jmax(fabs(unL) + cL, fabs(unR) + cR);
   const double hl = 0.5 * lam;
   out[0] = 0.5 * (fL0 + fR0) - hl * (uR[0] - uL[0]);
@@ -84,23 +89,28 @@ FRG_DEV void rusanov2(double gamma, double g1, const double uL[4], const double 
   out[3] = 0.5 * (fL3 + fR3) - hl * (uR[3] - uL[3]);
 }
 
-// HLLC normal flux, hllc_flux_n, src/flux/HLLC.jl:72-148.
+// HLLC normal flux, hllc_flux_n, src/flux/HLLC.jl:72-148.  `unit` skips the
+// renormalisation of an exactly unit normal (affine faces: (+-1,0), (0,+-1)).
 FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[4], double nxi,
-                   double nyi, double out[4]) {
-  const double nrm = sqrt(nxi * nxi + nyi * nyi);
-  if (nrm < kEps) {
-    rusanov2(gamma, g1, uL, uR, nxi, nyi, out);
-    return;
+                   double nyi, double out[4], bool unit = false) {
+  double nx = nxi, ny = nyi;
+  if (!unit) {
+    const double nrm = sqrt(nxi * nxi + nyi * nyi);
+    if (nrm < kEps) {
+      rusanov2(gamma, g1, uL, uR, nxi, nyi, out);
+      return;
+    }
+    const double rn = 1.0 / nrm;
+    nx = nxi * rn;
+    ny = nyi * rn;
   }
-  const double rn = 1.0 / nrm;
-  const double nx = nxi * rn, ny = nyi * rn;
-  const double rL = jmax(uL[0], kEps), riL = 1.0 / rL;
-  const double rR = jmax(uR[0], kEps), riR = 1.0 / rR;
+  const double rL = jfloor(uL[0], kEps), riL = 1.0 / rL;
+  const double rR = jfloor(uR[0], kEps), riR = 1.0 / rR;
   const double uLv = uL[1] * riL, vLv = uL[2] * riL;
   const double uRv = uR[1] * riR, vRv = uR[2] * riR;
   const double pLu = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
   const double pRu = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
-  const double pL = jmax(pLu, kEps), pR = jmax(pRu, kEps);
+  const double pL = jfloor(pLu, kEps), pR = jfloor(pRu, kEps);
   const double unL = uLv * nx + vLv * ny, unR = uRv * nx + vRv * ny;
   const double cL = sqrt(gamma * pL * riL), cR = sqrt(gamma * pR * riR);
   const double SL = jmin(unL - cL, unR - cR);
@@ -136,8 +146,10 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
   const double ustar = (u - un * nx) + SM * nx;
   const double vstar = (v - un * ny) + SM * ny;
   const double Sun = S - un;
-  const double factor = r * Sun / (S - SM);
-  const double estar = U[3] * ri + (SM - un) * (SM + p / (r * Sun));
+  // the two remaining divisions are independent reciprocals
+  const double rB = 1.0 / (S - SM), rA = 1.0 / (r * Sun);
+  const double factor = r * Sun * rB;
+  const double estar = U[3] * ri + (SM - un) * (SM + p * rA);
   out[0] = F0 + S * (factor - U[0]);
   out[1] = F1 + S * (factor * ustar - U[1]);
   out[2] = F2 + S * (factor * vstar - U[2]);
@@ -146,16 +158,16 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
 
 template <int FLUX>
 FRG_DEV void iflux2(double gamma, double g1, const double uL[4], const double uR[4], double nx,
-                    double ny, double out[4]) {
+                    double ny, double out[4], bool unit = false) {
   if (FLUX == FRG_FLUX_HLLC)
-    hllc2(gamma, g1, uL, uR, nx, ny, out);
+    hllc2(gamma, g1, uL, uR, nx, ny, out, unit);
   else
     rusanov2(gamma, g1, uL, uR, nx, ny, out);
 }
 
 // reflect_conserved (2D), BoundaryConditions.jl:43-60
 FRG_DEV void reflect2(const double U[4], double nx, double ny, double out[4]) {
-  const double r = jmax(U[0], kEps), ri = 1.0 / r;
+  const double r = jfloor(U[0], kEps), ri = 1.0 / r;
   const double u = U[1] * ri, v = U[2] * ri;
   const double un = u * nx + v * ny;
   out[0] = r;

@@ -148,6 +148,8 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
   const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
 
   // ---------------------------------------------------------------- slots
+  // element ids first (integer work only), so the tile copies can be issued
+  // before any metadata load
   for (int s = tid; s < NSLOT; s += NT) {
     const int bx = s % BX, by = s / BX;
     const bool corner = (bx == 0 || bx == BX - 1) && (by == 0 || by == BY - 1);
@@ -170,15 +172,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
         el = gy * nx + gx;
         if (ownpos && !wrap) fl |= kSlotOwn;
         if (wrap) fl |= kSlotWrap;
-        if (M.solid && M.solid[el]) fl |= kSlotSolid;
         if (prime && !(fl & kSlotOwn)) el = -1;  // prime/sense: own elements only
-      }
-      if (el >= 0) {
-        sJx[s] = M.Jx[gx];
-        sJy[s] = M.Jy[gy];
-        sDx[s] = M.dx[gx];
-        sDy[s] = M.dy[gy];
-        sEps[s] = (kAV && !prime) ? B.eps_in[el] : 0.0;
       }
     }
     sEl[s] = el;
@@ -214,8 +208,20 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
       }
     }
     cp_async_commit();
-    cp_async_wait<1>();
   }
+  // slot metadata while the copies are in flight
+  for (int s = tid; s < NSLOT; s += NT) {
+    const int el = sEl[s];
+    if (el < 0) continue;
+    const int gx = el % nx, gy = el / nx;
+    sJx[s] = M.Jx[gx];
+    sJy[s] = M.Jy[gy];
+    sDx[s] = M.dx[gx];
+    sDy[s] = M.dy[gy];
+    sEps[s] = (kAV && !prime) ? B.eps_in[el] : 0.0;
+    if (M.solid && M.solid[el]) sFlag[s] |= kSlotSolid;
+  }
+  cp_async_wait<1>();
   __syncthreads();
 
   if (!prime) {
@@ -339,9 +345,9 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
           double ug[4];
           reflect2(ui, nxo, nyo, ug);
           if (fluidB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh);
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !M.curved);
           else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh);
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !M.curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         } else {
@@ -355,7 +361,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
             nny = vert ? 0.0 : 1.0;
             sJ = vert ? sJy[sA] : sJx[sA];
           }
-          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh);
+          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh, !M.curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
@@ -402,9 +408,9 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
           double ug[4];
           exterior<4>(bc, ui, nxo, nyo, X, tstage, ug);
           if (haveB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh);
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !M.curved);
           else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh);
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !M.curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
