@@ -108,6 +108,8 @@ SIGNATURES = {
     "frg_get_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "frg_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp]),
+    "frg_residual2d_noalloc": (C.c_int, [C.POINTER(frg_solve_desc), C.c_void_p, C.c_void_p,
+                                         C.c_double, C.c_void_p]),
 }
 
 _lib = None

@@ -28,6 +28,9 @@ extern "C" {
 
 #define FRG_ABI_VERSION 1
 #define FRG_MAX_NP 6 /* P <= 5 */
+/* size limits of frg_residual2d_noalloc's fixed device scratch */
+#define FRG_NOALLOC_MAX_ELEMENTS 262144
+#define FRG_NOALLOC_MAX_SIDE 4096
 
 /* Status codes.  Numerical statuses mirror :ok / :diverged / :max_steps
    (src/time/SSP_RK3.jl:44-64, :110-117). */
@@ -208,6 +211,21 @@ int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt,
 int frg_get_variant(const frg_solve* s, int* variant, int* n_variants);
 int frg_set_variant(frg_solve* s, int variant);
 int frg_autotune(frg_solve* s, int reps, int* best, double* ms);
+
+/* Allocation-free residual evaluation (no counterpart in the reference).
+   Same result as frg_residual for a 2D affine mesh without solid mask, for
+   callers that cannot call cudaMalloc when they need a residual -- e.g. a
+   host framework whose device memory is owned by its own pool or budget.
+   u (input state) and du (output) are DEVICE pointers of ndof doubles in
+   the Julia layout, owned by the caller; t is the state time; stream is a
+   cudaStream_t (NULL: legacy default stream).  All scratch lives in one
+   fixed __device__ array (at most FRG_NOALLOC_MAX_ELEMENTS elements,
+   FRG_NOALLOC_MAX_SIDE per side; larger meshes return FRG_ERR_INVALID_ARG).
+   The first call on a device resolves that array's address: make it before
+   any stream capture.  Calls share the array: calls that overlap on the GPU
+   race and must be serialised by the caller.  Returns after enqueueing. */
+int frg_residual2d_noalloc(const frg_solve_desc* desc, const double* u, double* du,
+                           double t, void* stream);
 
 /* Instrumented frg_advance for profiling (no reference counterpart): runs
    nsteps steps with direct launches and times every stage kernel with CUDA
