@@ -16,6 +16,7 @@
 
 #include "frg_device.cuh"
 #include "frg_internal.h"
+#include "frg_runtime.h"
 
 namespace frg {
 int launch_stage2d_np2(const Launch2D&, const StageBufs&, cudaStream_t);
@@ -132,41 +133,10 @@ __global__ void step_end_kernel(DevScalars* sc, int nstages) {
 }  // namespace frg
 
 using namespace frg;
+using namespace frg::rt;
 
-struct frg_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-};
-
-struct frg_solve {
-  frg_ctx* ctx = nullptr;
-  int dim = 2, np = 0, nel = 0, neq = 4, nx = 0, ny = 1;
-  size_t ndof = 0;
-  int time_scheme = FRG_TIME_SSP_RK3;
-  int method = FRG_METHOD_NULL;
-  HostOps ops;
-  Launch2D L2{};
-  Launch1D L1{};
-  double* U[3] = {nullptr, nullptr, nullptr};
-  double* E[3] = {nullptr, nullptr, nullptr};
-  double* du = nullptr;
-  double* sigma = nullptr;
-  DevScalars* sc = nullptr;
-  DevScalars* hsc = nullptr;  // pinned host mirror
-  std::vector<void*> allocs;
-  size_t bytes = 0;
-  bool have_state = false;
-  int cur = 0;  // buffer index of the current state
-  double t = 0.0;
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  bool graph_lambda = false;
-  int64_t residual_evals = 0, steps = 0;
-  double hmin = 0.0;
-};
-
-namespace {
+namespace frg {
+namespace rt {
 
 int set_err(frg_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -337,6 +307,25 @@ int make_current_canonical(frg_solve* s) {
   return FRG_OK;
 }
 
+// Host mirror of the status word at the start of an integrate! call.
+void init_run_scalars(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps) {
+  DevScalars& h = *s->hsc;
+  h.t = s->t;
+  h.t_final = t_final;
+  h.cfl = cfl;
+  h.fixed_dt = fixed_dt;
+  h.hmin = s->hmin;
+  h.two_p1 = 2 * (s->np - 1) + 1;
+  h.status = kRunning;
+  h.active = 0;
+  h.flags = 0;
+  h.diverged_stage = 0;
+  h.lam_bits = 0ull;
+  h.n_steps = 0;
+  h.max_steps = max_steps;
+  h.residual_evals = s->residual_evals;
+}
+
 int finish_run(frg_solve* s) {
   int rc = pull_scalars(s);
   if (rc) return rc;
@@ -351,6 +340,12 @@ int finish_run(frg_solve* s) {
   }
   return FRG_OK;
 }
+
+}  // namespace rt
+}  // namespace frg
+
+namespace {
+using namespace frg::rt;
 
 int validate(frg_ctx* c, const frg_solve_desc* d) {
   if (!d) return set_err(c, FRG_ERR_INVALID_ARG, "null descriptor");
@@ -824,20 +819,7 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
   if (rc) return rc;
   const bool want_lambda = !(fixed_dt > 0.0);
   DevScalars& h = *s->hsc;
-  h.t = s->t;
-  h.t_final = t_final;
-  h.cfl = cfl;
-  h.fixed_dt = fixed_dt;
-  h.hmin = s->hmin;
-  h.two_p1 = 2 * (s->np - 1) + 1;
-  h.status = kRunning;
-  h.active = 0;
-  h.flags = 0;
-  h.diverged_stage = 0;
-  h.lam_bits = 0ull;
-  h.n_steps = 0;
-  h.max_steps = max_steps;
-  h.residual_evals = s->residual_evals;
+  init_run_scalars(s, t_final, cfl, fixed_dt, max_steps);
   if ((rc = push_scalars(s))) return rc;
   if ((rc = prime(s, 0, want_lambda))) return rc;
   // steps per graph: keep one graph launch around a few milliseconds of work

@@ -1,0 +1,65 @@
+// Runtime internals shared by the single-solve ABI (frforge_cuda.cu) and the
+// batched / served engine (frg_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "frg_internal.h"
+
+using frg::DevScalars;
+using frg::HostOps;
+using frg::Launch1D;
+using frg::Launch2D;
+
+struct frg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+};
+
+struct frg_solve {
+  frg_ctx* ctx = nullptr;
+  int dim = 2, np = 0, nel = 0, neq = 4, nx = 0, ny = 1;
+  size_t ndof = 0;
+  int time_scheme = FRG_TIME_SSP_RK3;
+  int method = FRG_METHOD_NULL;
+  HostOps ops;
+  Launch2D L2{};
+  Launch1D L1{};
+  double* U[3] = {nullptr, nullptr, nullptr};
+  double* E[3] = {nullptr, nullptr, nullptr};
+  double* du = nullptr;
+  double* sigma = nullptr;
+  DevScalars* sc = nullptr;
+  DevScalars* hsc = nullptr;  // pinned host mirror
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  bool have_state = false;
+  int cur = 0;  // buffer index of the current state
+  double t = 0.0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  bool graph_lambda = false;
+  int64_t residual_evals = 0, steps = 0;
+  double hmin = 0.0;
+};
+
+
+namespace frg {
+namespace rt {
+int set_err(frg_ctx* c, int code, const std::string& msg);
+int cuda_err(frg_ctx* c, cudaError_t e, const char* what);
+int push_scalars(frg_solve* s);
+int pull_scalars(frg_solve* s);
+int launch(frg_solve* s, const StageBufs& b);
+int prime(frg_solve* s, int buf, bool want_lambda);
+int finish_run(frg_solve* s);
+int make_current_canonical(frg_solve* s);
+void init_run_scalars(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps);
+}  // namespace rt
+__global__ void step_begin_kernel(DevScalars* sc);
+__global__ void step_end_kernel(DevScalars* sc, int nstages);
+}  // namespace frg

@@ -32,9 +32,10 @@ struct Smem1D {
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
 };
 
+// One tile of one stage; x0: first element of the tile.
 template <int NP, int FLUX, int AV>
-__global__ void __launch_bounds__(256)
-    stage1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const StageBufs B) {
+__device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev& M, const Phys& P,
+                                             const StageBufs& B, const int x0) {
   using S = Smem1D<NP>;
   constexpr int NEQ = 3, TX = S::TX, NSLOT = S::NSLOT;
   constexpr bool kBR0 = (AV == kAvBR0);
@@ -67,7 +68,6 @@ __global__ void __launch_bounds__(256)
   }
   (void)tstage;
   const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
-  const int x0 = blockIdx.x * TX;
 
   for (int s = tid; s < NSLOT; s += nthr) {
     int g = x0 + s - 1, el = -1, own = 0;
@@ -309,6 +309,13 @@ __global__ void __launch_bounds__(256)
     lam = jmax(lam, kEps);
     B.eps_out[el] = (sig > 0.0) ? P.c_av * sig * (sDx[s] / (double)P.pm) * lam : 0.0;
   }
+}
+
+// Single solve: the grid covers the mesh with tiles.
+template <int NP, int FLUX, int AV>
+__global__ void __launch_bounds__(256)
+    stage1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const StageBufs B) {
+  stage1d_tile<NP, FLUX, AV>(ops, M, P, B, blockIdx.x * Tile1D<NP>::TX);
 }
 
 }  // namespace frg

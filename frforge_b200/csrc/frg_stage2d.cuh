@@ -98,12 +98,12 @@ FRG_DEV void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// TX x TY: tile (elements); MINB: CTAs per SM the register budget targets;
-// U0S: u0 staged in shared memory.
-template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
-          bool U0S = true>
-__global__ void __launch_bounds__(kStageThreads, MINB)
-    stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
+// One tile of one stage.  TX x TY: tile (elements); MINB: CTAs per SM the
+// register budget targets (only sizes the static shared-memory check);
+// U0S: u0 staged in shared memory.  tx0, ty0: first element of the tile.
+template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S>
+__device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
+                                             const StageBufs& B, const int tx0, const int ty0) {
   using S = Smem2D<NP, TX, TY, U0S, MINB>;
   constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
   constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, NOWN = S::NOWN;
@@ -145,7 +145,6 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
   const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
   const bool need_u0 = (B.mode == kModeStage) && (B.stage != 1);
 
-  const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
 
   // ---------------------------------------------------------------- slots
   // element ids first (integer work only), so the tile copies can be issued
@@ -687,6 +686,14 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
       B.eps_out[el] = ev;
     }
   }
+}
+
+// Single solve: the grid covers the mesh with tiles.
+template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
+          bool U0S = true>
+__global__ void __launch_bounds__(kStageThreads, MINB)
+    stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
+  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
 }
 
 }  // namespace frg
