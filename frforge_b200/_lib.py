@@ -13,7 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfrforge_cuda.so")
 
 # status codes (frg_status)
-FRG_OK, FRG_DIVERGED, FRG_MAX_STEPS = 0, 1, 2
+FRG_OK, FRG_DIVERGED, FRG_MAX_STEPS, FRG_RUNNING = 0, 1, 2, 3
 FRG_ERR_INVALID_ARG, FRG_ERR_UNSUPPORTED_HOOK, FRG_ERR_OOM = -1, -2, -3
 FRG_ERR_CUDA, FRG_ERR_TIMEOUT, FRG_ERR_STATE = -4, -5, -6
 
@@ -24,7 +24,8 @@ BC_KIND = {"periodic": 0, "transmissive": 1, "dirichlet": 2, "reflecting": 3, "x
 METHOD = {"null": 0, "persson": 1}
 AV_FORM = {"conservative_br0": 0, "element_local_DD": 1}
 GEOM = {"affine": 0, "wavy": 1, "metrics": 2}
-STATUS_SYMBOL = {FRG_OK: "ok", FRG_DIVERGED: "diverged", FRG_MAX_STEPS: "max_steps"}
+STATUS_SYMBOL = {FRG_OK: "ok", FRG_DIVERGED: "diverged", FRG_MAX_STEPS: "max_steps",
+                 FRG_RUNNING: "running"}
 
 _dp = C.POINTER(C.c_double)
 
@@ -110,6 +111,15 @@ SIGNATURES = {
     "frg_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp]),
     "frg_residual2d_noalloc": (C.c_int, [C.POINTER(frg_solve_desc), C.c_void_p, C.c_void_p,
                                          C.c_double, C.c_void_p]),
+    "frg_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "frg_batch_destroy": (C.c_int, [C.c_void_p]),
+    "frg_batch_add": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(C.c_int)]),
+    "frg_batch_remove": (C.c_int, [C.c_void_p, C.c_int]),
+    "frg_batch_get_solve": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "frg_batch_start": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_int64]),
+    "frg_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_result), C.POINTER(C.c_int)]),
+    "frg_solve_bytes": (C.c_int, [C.POINTER(frg_solve_desc), C.POINTER(C.c_size_t)]),
 }
 
 _lib = None

@@ -138,6 +138,32 @@ struct Phys {
 
 enum : int { kAvNone = 0, kAvBR0 = 1, kAvDD = 2 };
 
+// static shared memory the batched stage kernels hold for their descriptors
+constexpr int kBatchStaticSmem = 1024;
+
+// One instance of a batch, as the batched kernels see it.
+struct BatchInst {
+  Mesh2Dev M2;  // dim == 2
+  Mesh1Dev M1;  // dim == 1
+  Phys P;
+  double* U[3];
+  double* E[3];
+  DevScalars* sc;
+  int rk2;
+  int dim;
+};
+// A tile of one instance: first element (x0, y0) of a TX x TY tile.
+struct BatchTile {
+  int inst, x0, y0, pad;
+};
+// Per-instance outcome gathered for the host in one copy.
+struct BatchStatus {
+  int status;
+  int active;
+  long long n_steps;
+  double t;
+};
+
 // ---- host helpers (frg_host.cpp) ----
 int build_host_ops(int p, int points, HostOps* out);
 int host_ops_from_caller(const frg_operators* in, HostOps* out);
@@ -162,6 +188,12 @@ struct Launch1D {
 };
 // Returns 0 or a CUDA error code.
 int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream);
+// batched stage launch over a group's tile list (same NP, flux, AV, tables)
+int launch_batch2d(const HostOps* ops, int flux, int av, int variant, const BatchInst* insts,
+                   const BatchTile* tiles, int ntiles, int stage, int mode, void* stream);
+int launch_batch1d(const HostOps* ops, int flux, int av, const BatchInst* insts,
+                   const BatchTile* tiles, int ntiles, int stage, int mode, void* stream);
+int batch_tile_shape(int dim, int np, int variant, int* tx, int* ty);
 int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream);
 int stage2d_variants(int np);
 

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include "frg_batch.cuh"
 #include "frg_stage1d.cuh"
 #include "frg_stage2d.cuh"
 
@@ -32,7 +33,8 @@ OpsT<NP> make_ops(const HostOps& h) {
 }
 
 // Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory).
-// Variant 0 is the default; the autotuner times all of them on the solve.
+// Variant 0 is the default, the fastest measured on a B200 for large meshes
+// (P=3: 512^2, P=4/5: 384^2); the autotuner times all of them on the solve.
 template <int NP>
 struct Variants2D;
 template <>
@@ -40,38 +42,38 @@ struct Variants2D<2> {
   static constexpr int n = 2;
   template <int V> struct V_;
 };
-template <> template <> struct Variants2D<2>::V_<0> { static constexpr int TX = 8, TY = 8, MINB = 2; static constexpr bool U0S = true; };
-template <> template <> struct Variants2D<2>::V_<1> { static constexpr int TX = 8, TY = 4, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<2>::V_<0> { static constexpr int TX = 8, TY = 8, MINB = 2; static constexpr bool U0S = true; };
+template <> struct Variants2D<2>::V_<1> { static constexpr int TX = 8, TY = 4, MINB = 3; static constexpr bool U0S = false; };
 template <>
 struct Variants2D<3> {
   static constexpr int n = 3;
   template <int V> struct V_;
 };
-template <> template <> struct Variants2D<3>::V_<0> { static constexpr int TX = 8, TY = 6, MINB = 2; static constexpr bool U0S = true; };
-template <> template <> struct Variants2D<3>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> template <> struct Variants2D<3>::V_<2> { static constexpr int TX = 4, TY = 4, MINB = 4; static constexpr bool U0S = false; };
+template <> struct Variants2D<3>::V_<0> { static constexpr int TX = 8, TY = 6, MINB = 2; static constexpr bool U0S = true; };
+template <> struct Variants2D<3>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<3>::V_<2> { static constexpr int TX = 4, TY = 4, MINB = 4; static constexpr bool U0S = false; };
 template <>
 struct Variants2D<4> {
   static constexpr int n = 3;
   template <int V> struct V_;
 };
-template <> template <> struct Variants2D<4>::V_<0> { static constexpr int TX = 8, TY = 4, MINB = 2; static constexpr bool U0S = true; };
-template <> template <> struct Variants2D<4>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> template <> struct Variants2D<4>::V_<2> { static constexpr int TX = 8, TY = 2, MINB = 4; static constexpr bool U0S = false; };
+template <> struct Variants2D<4>::V_<0> { static constexpr int TX = 8, TY = 2, MINB = 4; static constexpr bool U0S = false; };
+template <> struct Variants2D<4>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<4>::V_<2> { static constexpr int TX = 8, TY = 4, MINB = 2; static constexpr bool U0S = true; };
 template <>
 struct Variants2D<5> {
   static constexpr int n = 2;
   template <int V> struct V_;
 };
-template <> template <> struct Variants2D<5>::V_<0> { static constexpr int TX = 4, TY = 4, MINB = 2; static constexpr bool U0S = true; };
-template <> template <> struct Variants2D<5>::V_<1> { static constexpr int TX = 4, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<5>::V_<0> { static constexpr int TX = 4, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<5>::V_<1> { static constexpr int TX = 4, TY = 4, MINB = 2; static constexpr bool U0S = true; };
 template <>
 struct Variants2D<6> {
   static constexpr int n = 2;
   template <int V> struct V_;
 };
-template <> template <> struct Variants2D<6>::V_<0> { static constexpr int TX = 4, TY = 3, MINB = 2; static constexpr bool U0S = true; };
-template <> template <> struct Variants2D<6>::V_<1> { static constexpr int TX = 3, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<6>::V_<0> { static constexpr int TX = 3, TY = 3, MINB = 3; static constexpr bool U0S = false; };
+template <> struct Variants2D<6>::V_<1> { static constexpr int TX = 4, TY = 3, MINB = 2; static constexpr bool U0S = true; };
 
 template <int NP, int FLUX, int AV, int V>
 int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
@@ -152,6 +154,119 @@ int launch1d_np(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
   }
 }
 
+template <int NP, int FLUX, int AV, int V>
+int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles, int ntiles, int stage,
+                int mode, cudaStream_t st) {
+  using VV = typename Variants2D<NP>::template V_<V>;
+  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB>;
+  auto kern = stage2d_batch_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    if (e != cudaSuccess) return (int)e;
+    configured = true;
+  }
+  if (ntiles > 0) kern<<<ntiles, kStageThreads, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
+  return (int)cudaGetLastError();
+}
+
+template <int NP, int FLUX, int AV>
+int batch2d_inst(const HostOps& h, int variant, const BatchInst* insts, const BatchTile* tiles, int ntiles,
+                 int stage, int mode, cudaStream_t st) {
+  const int v = (variant >= 0 && variant < Variants2D<NP>::n) ? variant : 0;
+  switch (v) {
+    case 1:
+      if constexpr (Variants2D<NP>::n > 1) return batch2d_var<NP, FLUX, AV, 1>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    case 2:
+      if constexpr (Variants2D<NP>::n > 2) return batch2d_var<NP, FLUX, AV, 2>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    default:
+      break;
+  }
+  return batch2d_var<NP, FLUX, AV, 0>(h, insts, tiles, ntiles, stage, mode, st);
+}
+
+template <int NP>
+int batch2d_np(const HostOps& h, int flux, int av, int variant, const BatchInst* insts, const BatchTile* tiles,
+               int ntiles, int stage, int mode, cudaStream_t st) {
+  const bool hllc = flux == FRG_FLUX_HLLC;
+  switch (av) {
+    case kAvBR0:
+      return hllc ? batch2d_inst<NP, FRG_FLUX_HLLC, kAvBR0>(h, variant, insts, tiles, ntiles, stage, mode, st)
+                  : batch2d_inst<NP, FRG_FLUX_RUSANOV, kAvBR0>(h, variant, insts, tiles, ntiles, stage, mode, st);
+    case kAvDD:
+      return hllc ? batch2d_inst<NP, FRG_FLUX_HLLC, kAvDD>(h, variant, insts, tiles, ntiles, stage, mode, st)
+                  : batch2d_inst<NP, FRG_FLUX_RUSANOV, kAvDD>(h, variant, insts, tiles, ntiles, stage, mode, st);
+    default:
+      return hllc ? batch2d_inst<NP, FRG_FLUX_HLLC, kAvNone>(h, variant, insts, tiles, ntiles, stage, mode, st)
+                  : batch2d_inst<NP, FRG_FLUX_RUSANOV, kAvNone>(h, variant, insts, tiles, ntiles, stage, mode, st);
+  }
+}
+
+template <int NP, int FLUX, int AV>
+int batch1d_inst(const HostOps& h, const BatchInst* insts, const BatchTile* tiles, int ntiles, int stage,
+                 int mode, cudaStream_t st) {
+  using S = Smem1D<NP>;
+  auto kern = stage1d_batch_kernel<NP, FLUX, AV>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    if (e != cudaSuccess) return (int)e;
+    configured = true;
+  }
+  if (ntiles > 0) kern<<<ntiles, 256, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
+  return (int)cudaGetLastError();
+}
+
+template <int NP>
+int batch1d_np(const HostOps& h, int flux, int av, const BatchInst* insts, const BatchTile* tiles, int ntiles,
+               int stage, int mode, cudaStream_t st) {
+  const bool hllc = flux == FRG_FLUX_HLLC;
+  switch (av) {
+    case kAvBR0:
+      return hllc ? batch1d_inst<NP, FRG_FLUX_HLLC, kAvBR0>(h, insts, tiles, ntiles, stage, mode, st)
+                  : batch1d_inst<NP, FRG_FLUX_RUSANOV, kAvBR0>(h, insts, tiles, ntiles, stage, mode, st);
+    case kAvDD:
+      return hllc ? batch1d_inst<NP, FRG_FLUX_HLLC, kAvDD>(h, insts, tiles, ntiles, stage, mode, st)
+                  : batch1d_inst<NP, FRG_FLUX_RUSANOV, kAvDD>(h, insts, tiles, ntiles, stage, mode, st);
+    default:
+      return hllc ? batch1d_inst<NP, FRG_FLUX_HLLC, kAvNone>(h, insts, tiles, ntiles, stage, mode, st)
+                  : batch1d_inst<NP, FRG_FLUX_RUSANOV, kAvNone>(h, insts, tiles, ntiles, stage, mode, st);
+  }
+}
+
+template <int NP>
+int tile_shape_np(int dim, int variant, int* tx, int* ty) {
+  if (dim == 1) {
+    *tx = Tile1D<NP>::TX;
+    *ty = 1;
+    return 0;
+  }
+  const int v = (variant >= 0 && variant < Variants2D<NP>::n) ? variant : 0;
+  switch (v) {
+    case 1:
+      if constexpr (Variants2D<NP>::n > 1) {
+        *tx = Variants2D<NP>::template V_<1>::TX;
+        *ty = Variants2D<NP>::template V_<1>::TY;
+        return 0;
+      }
+      break;
+    case 2:
+      if constexpr (Variants2D<NP>::n > 2) {
+        *tx = Variants2D<NP>::template V_<2>::TX;
+        *ty = Variants2D<NP>::template V_<2>::TY;
+        return 0;
+      }
+      break;
+    default:
+      break;
+  }
+  *tx = Variants2D<NP>::template V_<0>::TX;
+  *ty = Variants2D<NP>::template V_<0>::TY;
+  return 0;
+}
+
 template <int NP>
 int variants2d() {
   return Variants2D<NP>::n;
@@ -168,4 +283,15 @@ int variants2d() {
     return launch1d_np<NPV>(L, b, st);                                                       \
   }                                                                                          \
   int stage2d_variants_np##NPV() { return variants2d<NPV>(); }                                \
+  int launch_batch2d_np##NPV(const HostOps& h, int flux, int av, int variant, const BatchInst* insts, \
+                             const BatchTile* tiles, int ntiles, int stage, int mode, cudaStream_t st) { \
+    return batch2d_np<NPV>(h, flux, av, variant, insts, tiles, ntiles, stage, mode, st);     \
+  }                                                                                          \
+  int launch_batch1d_np##NPV(const HostOps& h, int flux, int av, const BatchInst* insts,     \
+                             const BatchTile* tiles, int ntiles, int stage, int mode, cudaStream_t st) { \
+    return batch1d_np<NPV>(h, flux, av, insts, tiles, ntiles, stage, mode, st);              \
+  }                                                                                          \
+  int tile_shape_np##NPV(int dim, int variant, int* tx, int* ty) {                           \
+    return tile_shape_np<NPV>(dim, variant, tx, ty);                                         \
+  }                                                                                          \
   }

@@ -80,7 +80,8 @@ struct Smem2D {
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2 + 8;
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
-  static_assert(MINB * (bytes + 1024) <= 228 * 1024, "MINB CTAs must fit in one SM's shared memory");
+  // 1 KB reserved per CTA plus the batched kernels' static descriptors
+  static_assert(MINB * (bytes + 1024 + kBatchStaticSmem) <= 228 * 1024, "MINB CTAs must fit in one SM's shared memory");
 };
 
 constexpr int kStageThreads = 256;

@@ -79,74 +79,83 @@ def _bc_struct(bc: AbstractBC) -> L.frg_bc:
     return b
 
 
+def make_desc(state, eq, method: Optional[AbstractCapturingMethod] = None, time: Optional[str] = None,
+              caller_ops=None):
+    """frg_solve_desc of a solution state + method; returns (desc, keep): keep
+    holds the host arrays the descriptor points into (alive until the solve is
+    created)."""
+    method = method or NullCapturing()
+    spec = method.gpu_spec()
+    d = L.frg_solve_desc()
+    keep = []
+    sch = state.scheme
+    d.dim = state.dim
+    d.p = state.ops.p
+    d.points = L.POINTS[sch.points]
+    d.flux = L.FLUX[sch.flux]
+    d.time_scheme = L.TIME[time or sch.time]
+    d.gamma = eq.gamma
+    m = state.mesh
+    xv = np.ascontiguousarray(m.x_vertices)
+    keep.append(xv)
+    d.x_vertices = L.dptr(xv)
+    if state.dim == 1:
+        d.nx, d.ny = m.n_elements, 1
+        d.x_left, d.x_right = m.x_left, m.x_right
+        d.bc[0] = _bc_struct(m.left_bc)
+        d.bc[1] = _bc_struct(m.right_bc)
+    else:
+        d.nx, d.ny = m.nx, m.ny
+        d.x_left, d.x_right, d.y_bottom, d.y_top = m.x_left, m.x_right, m.y_bottom, m.y_top
+        yv = np.ascontiguousarray(m.y_vertices)
+        keep.append(yv)
+        d.y_vertices = L.dptr(yv)
+        for k, bc in enumerate((m.left_bc, m.right_bc, m.bottom_bc, m.top_bc)):
+            d.bc[k] = _bc_struct(bc)
+        if m.solid is not None:
+            sol = np.ascontiguousarray(m.solid, dtype=np.uint8)
+            keep.append(sol)
+            d.solid = sol.ctypes.data_as(C.c_void_p)
+        if state.metrics is not None:
+            mt = L.frg_metrics2d()
+            for name in L._METRIC_FIELDS:
+                a = np.asfortranarray(state.metrics[name], dtype=np.float64).ravel(order="F")
+                a = np.ascontiguousarray(a)
+                keep.append(a)
+                setattr(mt, name, L.dptr(a))
+            keep.append(mt)
+            d.geometry = L.GEOM["metrics"]
+            d.metrics = C.pointer(mt)
+        elif state.wavy_amp is not None:
+            d.geometry = L.GEOM["wavy"]
+            d.wavy_amp = state.wavy_amp
+    if caller_ops is not None:
+        o = L.frg_operators()
+        o.p = caller_ops["p"] if isinstance(caller_ops, dict) else caller_ops.p
+        o.points = d.points
+        for name in ("xi", "w", "D", "l_L", "l_R", "gL_xi", "gR_xi", "V"):
+            src = caller_ops[name] if isinstance(caller_ops, dict) else getattr(
+                caller_ops, "V_legendre" if name == "V" else name)
+            a = np.ascontiguousarray(np.asarray(src, dtype=np.float64).ravel(order="F"))
+            keep.append(a)
+            setattr(o, name, L.dptr(a))
+        keep.append(o)
+        d.ops = C.pointer(o)
+    d.method = L.METHOD[spec["method"]]
+    d.av_form = L.AV_FORM[spec["av_form"]]
+    d.kappa, d.s0_factor, d.eps_floor, d.c_av = (spec["kappa"], spec["s0_factor"],
+                                                spec["eps_floor"], spec["c_av"])
+    return d, keep
+
+
 class GpuSolve:
     """A device-resident solve (frg_solve): descriptor, state buffers, graphs."""
 
     def __init__(self, state, eq, method: Optional[AbstractCapturingMethod] = None,
                  time: Optional[str] = None, ctx: Optional[Context] = None, caller_ops=None):
-        method = method or NullCapturing()
-        spec = method.gpu_spec()
         self.ctx = ctx or default_context()
         self.state_shape = state.u.shape
-        d = L.frg_solve_desc()
-        self._keep = []
-        sch = state.scheme
-        d.dim = state.dim
-        d.p = state.ops.p
-        d.points = L.POINTS[sch.points]
-        d.flux = L.FLUX[sch.flux]
-        d.time_scheme = L.TIME[time or sch.time]
-        d.gamma = eq.gamma
-        m = state.mesh
-        xv = np.ascontiguousarray(m.x_vertices)
-        self._keep.append(xv)
-        d.x_vertices = L.dptr(xv)
-        if state.dim == 1:
-            d.nx, d.ny = m.n_elements, 1
-            d.x_left, d.x_right = m.x_left, m.x_right
-            d.bc[0] = _bc_struct(m.left_bc)
-            d.bc[1] = _bc_struct(m.right_bc)
-        else:
-            d.nx, d.ny = m.nx, m.ny
-            d.x_left, d.x_right, d.y_bottom, d.y_top = m.x_left, m.x_right, m.y_bottom, m.y_top
-            yv = np.ascontiguousarray(m.y_vertices)
-            self._keep.append(yv)
-            d.y_vertices = L.dptr(yv)
-            for k, bc in enumerate((m.left_bc, m.right_bc, m.bottom_bc, m.top_bc)):
-                d.bc[k] = _bc_struct(bc)
-            if m.solid is not None:
-                sol = np.ascontiguousarray(m.solid, dtype=np.uint8)
-                self._keep.append(sol)
-                d.solid = sol.ctypes.data_as(C.c_void_p)
-            if state.metrics is not None:
-                mt = L.frg_metrics2d()
-                for name in L._METRIC_FIELDS:
-                    a = np.asfortranarray(state.metrics[name], dtype=np.float64).ravel(order="F")
-                    a = np.ascontiguousarray(a)
-                    self._keep.append(a)
-                    setattr(mt, name, L.dptr(a))
-                self._keep.append(mt)
-                d.geometry = L.GEOM["metrics"]
-                d.metrics = C.pointer(mt)
-            elif state.wavy_amp is not None:
-                d.geometry = L.GEOM["wavy"]
-                d.wavy_amp = state.wavy_amp
-        if caller_ops is not None:
-            o = L.frg_operators()
-            o.p = caller_ops["p"] if isinstance(caller_ops, dict) else caller_ops.p
-            o.points = d.points
-            for name in ("xi", "w", "D", "l_L", "l_R", "gL_xi", "gR_xi", "V"):
-                src = caller_ops[name] if isinstance(caller_ops, dict) else getattr(
-                    caller_ops, "V_legendre" if name == "V" else name)
-                a = np.ascontiguousarray(np.asarray(src, dtype=np.float64).ravel(order="F"))
-                self._keep.append(a)
-                setattr(o, name, L.dptr(a))
-            self._keep.append(o)
-            d.ops = C.pointer(o)
-        d.method = L.METHOD[spec["method"]]
-        d.av_form = L.AV_FORM[spec["av_form"]]
-        d.kappa, d.s0_factor, d.eps_floor, d.c_av = (spec["kappa"], spec["s0_factor"],
-                                                    spec["eps_floor"], spec["c_av"])
+        d, self._keep = make_desc(state, eq, method, time, caller_ops)
         self.desc = d
         h = C.c_void_p()
         L.check(L.load().frg_solve_create(self.ctx.handle, C.byref(d), C.byref(h)), self.ctx.handle,

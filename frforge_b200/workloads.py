@@ -117,3 +117,25 @@ class Workload2D:
 C2 = Workload2D("c2", 128, 4, "rusanov", "persson_av", 0.1, True, 0.1, 500)
 C3 = Workload2D("c3", 512, 3, "hllc", "persson_av", 0.1, False, 0.1, 1000)
 WORKLOADS = {"c2": C2, "c3": C3}
+
+
+def c4_instances(seed: int = DEFAULT_SEED, count: int = 64, steps: int = 200) -> List[Workload2D]:
+    """The batched workload: ``count`` independent 2D solves drawn from one
+    SplitMix64 stream, per instance in this order: n = round(exp(U[ln 16,
+    ln 256])) elements per side, P ~ U{1..5}, flux HLLC or Rusanov with
+    probability 1/2 each, c_av = 0.1 * U[0.5, 2].  Even instances are periodic
+    density waves, odd ones transmissive four-quadrant problems; each IC has
+    its own seed (seed + 1 + index).  Every instance runs ``steps`` SSP-RK3
+    steps at CFL 0.1 with Persson AV (BR0).  About 0.75 M elements and 54 M
+    DOF in total at the default size."""
+    g = splitmix64(seed)
+    out = []
+    for i in range(count):
+        n = int(round(math.exp(uniform(g, math.log(16.0), math.log(256.0)))))
+        p = 1 + min(int(5.0 * next(g)), 4)
+        flux = "hllc" if next(g) < 0.5 else "rusanov"
+        c_av = 0.1 * uniform(g, 0.5, 2.0)
+        periodic = i % 2 == 0
+        out.append(Workload2D("c2" if periodic else "c3", n, p, flux, "persson_av", c_av, periodic, 0.1,
+                              steps, seed=seed + 1 + i))
+    return out

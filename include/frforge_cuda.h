@@ -38,6 +38,7 @@ typedef enum {
   FRG_OK = 0,
   FRG_DIVERGED = 1,
   FRG_MAX_STEPS = 2,
+  FRG_RUNNING = 3,               /* batched instance still advancing */
   FRG_ERR_INVALID_ARG = -1,      /* ArgumentError in the reference */
   FRG_ERR_UNSUPPORTED_HOOK = -2, /* a capturing hook with no GPU implementation */
   FRG_ERR_OOM = -3,              /* device allocation / admission budget */
@@ -146,6 +147,7 @@ typedef struct {
 
 typedef struct frg_ctx frg_ctx;
 typedef struct frg_solve frg_solve;
+typedef struct frg_batch frg_batch;
 
 /* ---- library / context ---------------------------------------------- */
 int frg_abi_version(void);
@@ -233,6 +235,43 @@ int frg_residual2d_noalloc(const frg_solve_desc* desc, const double* u, double* 
    stage-(k+1) kernel, k = 0..2 (stage 3 unused for SSP-RK2). */
 int frg_time_stages(frg_solve* s, int64_t nsteps, double cfl, double fixed_dt,
                     double* stage_ms, frg_result* out);
+
+/* ---------------------------------------------------------------- batches
+   Many independent solves advanced together on one GPU (no counterpart in
+   the reference, whose callers -- case sweeps, robustness matrices, the
+   invent/confirm loop (src/invent/Robustness.jl:245, src/invent/Confirm.jl:35)
+   -- call integrate! (src/time/Integrate.jl:9) once per case, one after the
+   other).  Every instance is an ordinary solve with its own state, mesh,
+   tables, dt, time and status; its results are bit-identical to the same
+   solve advanced alone with frg_advance.  Each stage launches one kernel per
+   group of instances that share (dim, P, flux, dissipation form, tables),
+   over the ragged list of that group's tiles; K steps are captured in one
+   CUDA graph.  Adding or removing instances takes effect at the next
+   frg_batch_run (continuous batching). */
+
+/* capacity: instance slots; hbm_budget: admission limit in bytes on the
+   instances' device memory (0 = none). */
+int frg_batch_create(frg_ctx* ctx, int capacity, size_t hbm_budget, frg_batch** out);
+int frg_batch_destroy(frg_batch* b); /* destroys its instances too */
+/* Create an instance in a free slot (*slot).  FRG_ERR_OOM when the batch is
+   full or the HBM budget would be exceeded.  The instance is idle until
+   frg_batch_start. */
+int frg_batch_add(frg_batch* b, const frg_solve_desc* desc, int* slot);
+int frg_batch_remove(frg_batch* b, int slot);
+/* The instance's solve: frg_upload_state / frg_download_state /
+   frg_residual work on it while it is not running. */
+int frg_batch_get_solve(frg_batch* b, int slot, frg_solve** s);
+/* Start an instance's run with integrate!'s arguments (as frg_advance). */
+int frg_batch_start(frg_batch* b, int slot, double t_final, double cfl, double fixed_dt,
+                    int64_t max_steps);
+/* Advance every running instance by up to max_steps steps, or until none
+   runs.  results (capacity entries, may be NULL): per slot FRG_OK /
+   FRG_DIVERGED / FRG_MAX_STEPS when the run ended, FRG_RUNNING while it
+   goes on, FRG_ERR_STATE for an empty slot; n_steps and t of the run. */
+int frg_batch_run(frg_batch* b, int64_t max_steps, frg_result* results, int* n_running);
+/* Upper bound of the device bytes a solve of this descriptor holds (the
+   admission test of a served batch). */
+int frg_solve_bytes(const frg_solve_desc* desc, size_t* bytes);
 
 #ifdef __cplusplus
 }

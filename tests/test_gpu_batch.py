@@ -1,0 +1,266 @@
+"""Batched execution (frg_batch_*).
+
+* An instance's result does not depend on the rest of the batch: every
+  instance of a mixed batch, including ones that join or leave between runs,
+  ends bit-identical to the same instance run alone in a batch.
+* The batched kernels agree with the single-solve path (frg_advance, itself
+  checked against the oracle in test_gpu_parity.py) to 1e-10 relative L-inf
+  with identical status and step count.  They are not bitwise equal to it:
+  the two kernels read the mesh and stage descriptors from different memory
+  (shared memory vs kernel parameters), so the compiler fuses a few
+  multiply-adds differently.
+* One batched instance is checked against the oracle directly."""
+import numpy as np
+import pytest
+
+import frforge_b200 as F
+from frforge_b200 import _lib as L
+from frforge_b200.batch import Batch, solve_bytes
+
+from pairs import (four_quadrant_state, pair_1d, pair_2d, prim2cons1, rel_linf, smooth_state_2d)
+
+pytestmark = pytest.mark.gpu
+
+
+def _sod(orc):
+    orc.ic_sod()
+    return orc.u.copy()
+
+
+# (builder kwargs, IC, run arguments)
+MIX = [
+    (dict(dim=2, p=1, nx=12, ny=12, flux="rusanov", method="persson"), "smooth",
+     dict(t_final=1.0, cfl=0.1, max_steps=40)),
+    (dict(dim=2, p=3, nx=20, ny=20, flux="hllc", method="persson", bcs=("transmissive",) * 4), "quad",
+     dict(t_final=1.0, cfl=0.1, max_steps=35)),
+    (dict(dim=2, p=3, nx=13, ny=9, flux="hllc", method="persson", bcs=("transmissive",) * 4), "quad",
+     dict(t_final=0.02, cfl=0.1, max_steps=1000)),
+    (dict(dim=2, p=4, nx=10, ny=14, flux="rusanov", time="ssp_rk2", method="persson",
+          av_form="element_local_DD"), "smooth", dict(t_final=0.03, dt=1e-3, max_steps=1000)),
+    (dict(dim=2, p=5, nx=8, ny=8, flux="rusanov", method="null"), "smooth",
+     dict(t_final=1.0, cfl=0.1, max_steps=25)),
+    (dict(dim=2, p=2, nx=12, ny=12, flux="rusanov", method="persson", wavy=1), "smooth",
+     dict(t_final=1.0, cfl=0.1, max_steps=30)),
+    (dict(dim=2, p=2, nx=16, ny=8, flux="hllc", method="persson",
+          bcs=("reflecting", "transmissive", ("dirichlet", (1.0, 0.3, 0.0, 2.0)), "reflecting")), "quad",
+     dict(t_final=1.0, cfl=0.1, max_steps=30)),
+    (dict(dim=1, p=2, nel=64, method="persson"), "sod", dict(t_final=0.05, cfl=0.15, max_steps=10**6)),
+    (dict(dim=1, p=3, nel=100, time="ssp_rk2", method="null", left="periodic", right="periodic"),
+     "wave1d", dict(t_final=1.0, cfl=0.1, max_steps=45)),
+]
+
+
+def _build(kw):
+    kw = dict(kw)
+    dim = kw.pop("dim")
+    return (pair_2d if dim == 2 else pair_1d)(**kw)
+
+
+def _ic(orc, name, seed):
+    if name == "smooth":
+        return smooth_state_2d(orc, seed=seed)
+    if name == "quad":
+        return four_quadrant_state(orc, seed=seed, jump_scale=0.25)
+    if name == "sod":
+        return _sod(orc)
+    x = orc.coords()
+    return prim2cons1(1.0 + 0.2 * np.sin(2 * np.pi * x), 1.0 + 0 * x, 1.0 + 0 * x)
+
+
+def _run_alone(solve, u0, run):
+    solve.upload(u0, 0.0)
+    r = solve.advance(run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+    u, t = solve.download()
+    return r, u, t
+
+
+def _close(u, u_ref, tol=1e-10):
+    nan = np.isnan(u_ref)
+    assert np.array_equal(np.isnan(u), nan)
+    if nan.all():
+        return
+    assert rel_linf(np.where(nan, 0.0, u), np.where(nan, 0.0, u_ref)) <= tol
+
+
+def _solo(state, kw, run):
+    """The instance run alone in a batch: the bitwise reference of the mix."""
+    b = Batch(capacity=1)
+    i = b.add(state, _eq(kw), _method(kw))
+    b.start(i, run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+    r = b.run()[i]
+    u, t = b.download(i)
+    b.close()
+    return r, u, t
+
+
+def _setup(cases, seed0=11):
+    out = []
+    for k, (kw, ic, run) in enumerate(cases):
+        orc, state, solve = _build(kw)
+        u0 = _ic(orc, ic, seed0 + k)
+        state.u[...] = u0
+        state.t = 0.0
+        out.append((orc, state, solve, u0, run, kw))
+    return out
+
+
+def _method(kw):
+    if kw.get("method", "null") == "null":
+        return F.NullCapturing()
+    return F.PerssonAVMethod(c_av=kw.get("c_av", 0.1), av_form=kw.get("av_form", "conservative_br0"))
+
+
+def _eq(kw):
+    return F.Euler2D(1.4) if kw["dim"] == 2 else F.Euler1D(1.4)
+
+
+def test_batch_mix_matches_solo_bitwise_and_single_path():
+    items = _setup(MIX)
+    single = [_run_alone(solve, u0, run) for (_, _, solve, u0, run, _) in items]
+    solo = [_solo(state, kw, run) for (_, state, _, _, run, kw) in items]
+    b = Batch(capacity=len(items) + 3)
+    slots = []
+    for (orc, state, solve, u0, run, kw) in items:
+        i = b.add(state, _eq(kw), _method(kw))
+        b.start(i, run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+        slots.append(i)
+    res = b.run()
+    assert b.n_running == 0
+    for k, i in enumerate(slots):
+        r = res[i]
+        u, t = b.download(i)
+        # in the mix == alone in a batch, bit for bit
+        r_solo, u_solo, t_solo = solo[k]
+        assert r == r_solo, k
+        assert t == t_solo and np.array_equal(u, u_solo), k
+        # == the single-solve path to 1e-10
+        r_one, u_one, t_one = single[k]
+        assert r["status"] == r_one["status"] and r["n_steps"] == r_one["n_steps"], k
+        assert t == pytest.approx(t_one, rel=1e-13, abs=1e-15), k
+        _close(u, u_one)
+    # empty slots report None
+    assert all(res[k] is None for k in range(len(items), len(items) + 3))
+    b.close()
+
+
+def test_batched_instance_matches_oracle():
+    # Sod P=2 Ne=64 with Persson AV to t = 0.2, inside a batch with a 2D case
+    orc, state, solve = pair_1d(p=2, nel=64, method="persson", c_av=0.1)
+    u0 = _sod(orc)
+    r_ref = orc.integrate(0.2, cfl=0.15)
+    o2, st2, _ = pair_2d(p=3, nx=12, ny=12, flux="hllc", method="persson", bcs=("transmissive",) * 4)
+    st2.u[...] = four_quadrant_state(o2, jump_scale=0.25)
+    b = Batch(capacity=2)
+    state.u[...] = u0
+    i = b.add(state, F.Euler1D(1.4), F.PerssonAVMethod(c_av=0.1))
+    j = b.add(st2, F.Euler2D(1.4), F.PerssonAVMethod(c_av=0.1))
+    b.start(i, 0.2, cfl=0.15)
+    b.start(j, 1.0, cfl=0.1, max_steps=20)
+    res = b.run()
+    assert res[i]["status"] == "ok" and res[i]["n_steps"] == r_ref["n_steps"] == 950
+    assert res[j]["status"] == "max_steps" and res[j]["n_steps"] == 20
+    u, t = b.download(i)
+    assert t == pytest.approx(0.2, abs=1e-15)
+    assert np.sum(np.abs(u - orc.u)) / np.sum(np.abs(orc.u)) <= 1e-8
+    b.close()
+
+
+def test_continuous_batching_add_remove_midrun():
+    # instances join and leave between runs; each still ends bit-identical to
+    # its run alone
+    cases = [MIX[0], MIX[1], MIX[4], MIX[7], MIX[3]]
+    items = _setup(cases, seed0=31)
+    solo = [_solo(state, kw, run) for (_, state, _, _, run, kw) in items]
+    b = Batch(capacity=3)
+
+    def add_start(k):
+        orc, state, solve, u0, run, kw = items[k]
+        i = b.add(state, _eq(kw), _method(kw))
+        b.start(i, run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+        return i
+
+    def check(k, i, res):
+        r_solo, u_solo, t_solo = solo[k]
+        assert res[i] == r_solo, k
+        u, t = b.download(i)
+        assert t == t_solo and np.array_equal(u, u_solo), k
+
+    s0, s1 = add_start(0), add_start(1)
+    res = b.run(max_steps=7)
+    assert res[s0]["status"] == "running" and res[s0]["n_steps"] == 7
+    s2 = add_start(2)  # joins a running batch
+    res = b.run(max_steps=5)
+    assert res[s2]["n_steps"] == 5 and res[s0]["n_steps"] == 12
+    with pytest.raises(F.FRGError):
+        add_start(3)  # capacity 3: full
+    res = b.run()
+    for k, i in ((0, s0), (1, s1), (2, s2)):
+        check(k, i, res)
+    b.remove(s1)
+    s3 = add_start(3)  # reuses the freed slot
+    assert s3 == s1
+    b.remove(s0)
+    s4 = add_start(4)
+    res = b.run()
+    check(3, s3, res)
+    check(4, s4, res)
+    check(2, s2, res)  # a finished instance is left untouched by later runs
+    b.close()
+
+
+def test_divergent_instance_does_not_disturb_others():
+    items = _setup([MIX[0], MIX[7], MIX[4]], seed0=51)
+    # poison instance 1 (1D Sod) with a NaN
+    bad = items[1][3].copy()
+    bad[1, 5, 0] = np.nan
+    items[1] = items[1][:3] + (bad,) + items[1][4:]
+    items[1][1].u[...] = bad
+    single = [_run_alone(solve, u0, run) for (_, _, solve, u0, run, _) in items]
+    assert single[1][0]["status"] == "diverged"
+    solo = [_solo(state, kw, run) for (_, state, _, _, run, kw) in items]
+    b = Batch(capacity=3)
+    slots = []
+    for (orc, state, solve, u0, run, kw) in items:
+        i = b.add(state, _eq(kw), _method(kw))
+        b.start(i, run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+        slots.append(i)
+    res = b.run()
+    for k, i in enumerate(slots):
+        r_one = single[k][0]
+        assert res[i]["status"] == r_one["status"] and res[i]["n_steps"] == r_one["n_steps"]
+        assert res[i] == solo[k][0]
+        u, t = b.download(i)
+        assert t == solo[k][2]
+        assert np.array_equal(u, solo[k][1], equal_nan=True)
+        _close(u, single[k][1])
+    b.close()
+
+
+def test_hbm_budget_admission():
+    orc, state, solve = pair_2d(p=3, nx=32, ny=32, method="persson")
+    need = solve_bytes(state, F.Euler2D(1.4), F.PerssonAVMethod())
+    assert need >= solve.info()["device_bytes"]
+    b = Batch(capacity=8, hbm_budget=int(2.5 * need))
+    b.add(state, F.Euler2D(1.4), F.PerssonAVMethod())
+    b.add(state, F.Euler2D(1.4), F.PerssonAVMethod())
+    with pytest.raises(F.FRGError) as e:
+        b.add(state, F.Euler2D(1.4), F.PerssonAVMethod())
+    assert e.value.code == L.FRG_ERR_OOM
+    b.remove(0)
+    b.add(state, F.Euler2D(1.4), F.PerssonAVMethod())  # room again
+    b.close()
+
+
+def test_start_without_state_and_bad_slot():
+    orc, state, solve = pair_2d(p=2, nx=8, ny=8)
+    b = Batch(capacity=2)
+    with pytest.raises(ValueError):
+        b.start(1, 1.0)
+    with pytest.raises(ValueError):
+        b.remove(0)
+    i = b.add(state, F.Euler2D(1.4))
+    with pytest.raises(ValueError):
+        b.start(i, 1.0, cfl=0.0)
+    res = b.run()  # nothing running: returns at once
+    assert res[i]["status"] in ("ok", "max_steps") and b.n_running == 0
+    b.close()
