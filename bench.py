@@ -7,6 +7,7 @@ evaluations over all 512^2 x 16 x 4 = 16.8M degrees of freedom.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --workload batched     # 64 mixed solves, batched vs one at a time
+  python bench.py --workload served      # Poisson request trace, served vs one at a time
 
 ours: value = DOF-stage/s with the state resident in HBM, timed with CUDA
 events on the library's stream (max over ranks); e2e = the same metric through
@@ -409,6 +410,115 @@ def run_batched(args):
     return 0
 
 
+def run_served(args):
+    """A seeded Poisson request trace (frforge_b200.workloads.served_trace:
+    1D and 2D solves, P 1..5, wavy 2D meshes, t_final U[0.05, 0.25]) served by
+    frg_server_* against the same requests served one at a time (FIFO,
+    frg_solve_create + frg_advance + download per request).  Latency is
+    arrival -> final state on the host, on the host clock; both arms include
+    the device set-up of every solve (initial states are built beforehand)."""
+    import torch
+
+    import frforge_b200 as F
+    from frforge_b200.serve import Server
+    from frforge_b200.workloads import served_trace
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = F.Context(local)
+    trace = served_trace(count=args.served_requests)
+    built = [req.build(F) for req in trace]
+    arrivals = np.array([r.arrival for r in trace])
+
+    def served_arm():
+        srv = Server(slots=64, hbm_budget=64 << 30, steps_per_pump=8, ctx=ctx)
+        done_at, ids, res = {}, [], {}
+        nxt, t0 = 0, time.perf_counter()
+        while len(done_at) < len(trace):
+            now = time.perf_counter() - t0
+            while nxt < len(trace) and arrivals[nxt] <= now:
+                st, eq, m = built[nxt]
+                ids.append(srv.submit(st, eq, m, t_final=trace[nxt].t_final, cfl=trace[nxt].cfl))
+                nxt += 1
+            _, q, a = srv.pump()
+            now = time.perf_counter() - t0
+            for rid in srv.take_completed():
+                done_at[rid] = now
+                res[rid] = srv.result(rid)
+            if q == 0 and a == 0 and nxt < len(trace):
+                time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+        srv.close()
+        lat = np.array([done_at[rid] - arrivals[k] for k, rid in enumerate(ids)])
+        return lat, max(done_at.values()), [res[rid] for rid in ids]
+
+    def sequential_arm():
+        lat, res = [], []
+        t0 = time.perf_counter()
+        for k, req in enumerate(trace):
+            now = time.perf_counter() - t0
+            if arrivals[k] > now:
+                time.sleep(arrivals[k] - now)
+            st, eq, m = built[k]
+            s = F.GpuSolve(st, eq, m, ctx=ctx)
+            s.upload(st.u, 0.0)
+            r = s.advance(req.t_final, cfl=req.cfl)
+            u, _ = s.download()
+            s.close()
+            r["u"] = u
+            res.append(r)
+            lat.append(time.perf_counter() - t0 - arrivals[k])
+        return np.array(lat), time.perf_counter() - t0, res
+
+    with ClockSampler(local) as clk:
+        lat_s, span_s, res_s = served_arm()
+        lat_q, span_q, res_q = sequential_arm()
+    # The served path runs the batched kernels, the sequential one the
+    # single-solve kernels: they fuse a few multiply-adds differently, and over
+    # thousands of shocked steps that rounding grows.  Status and step count
+    # must agree; the states are compared in relative L1 (and L-inf reported).
+    worst, worst_l1 = 0.0, 0.0
+    for k, (a, c) in enumerate(zip(res_s, res_q)):
+        if a["status"] == c["status"] == "diverged":
+            continue  # blow-up: the step it is detected at is rounding-sensitive
+        if a["status"] != c["status"] or a["n_steps"] != c["n_steps"]:
+            raise RuntimeError(f"served request {k} ({trace[k]}) ended {a['status']} after {a['n_steps']} "
+                               f"steps, alone {c['status']} after {c['n_steps']}")
+        d = np.abs(a["u"] - c["u"])
+        worst = max(worst, float(d.max() / max(np.max(np.abs(c["u"])), 1e-300)))
+        worst_l1 = max(worst_l1, float(d.sum() / max(np.sum(np.abs(c["u"])), 1e-300)))
+    if worst_l1 > 1e-6:
+        raise RuntimeError(f"served results differ from the sequential ones (rel L1 {worst_l1:.3e})")
+    steps = sum(r["n_steps"] for r in res_s)
+    dof_stages = sum(3 * req.ndof * r["n_steps"] for req, r in zip(trace, res_s))
+    line = {
+        "metric": f"served solves/s and latency ({len(trace)}-request Poisson trace at 200 req/s) vs one at a time",
+        "value": len(trace) / span_s, "unit": "solves/s", "n_gpus": 1, "steps": int(steps),
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded request trace)",
+        "config": {"workload": "served: Poisson arrivals 200/s; 1D Ne~U{128..4096} or 2D n~U{16..384} "
+                               "(1/4 wavy, amplitude 0.05), P~U{1..5}, HLLC/Rusanov, density wave or "
+                               "Riemann IC (jumps x0.25), periodic, t_final~U[0.05,0.25], Persson AV, "
+                               "SSP-RK3, CFL 0.1",
+                   "requests": len(trace), "slots": 64, "steps_per_pump": 8},
+        "latency_s": {"p50": float(np.percentile(lat_s, 50)), "p99": float(np.percentile(lat_s, 99)),
+                      "max": float(lat_s.max())},
+        "sequential": {"value": len(trace) / span_q, "unit": "solves/s",
+                       "latency_s": {"p50": float(np.percentile(lat_q, 50)),
+                                     "p99": float(np.percentile(lat_q, 99)), "max": float(lat_q.max())}},
+        "speedup_vs_sequential": span_q / span_s,
+        "dof_stage_per_s": dof_stages / span_s,
+        "max_rel_linf_vs_sequential": worst,
+        "max_rel_l1_vs_sequential": worst_l1,
+        "statuses": {st: sum(1 for r in res_s if r["status"] == st) for st in sorted({r["status"] for r in res_s})},
+        "e2e": {"value": len(trace) / span_s, "unit": "solves/s",
+                "h2d_bytes_per_step": 8 * sum(req.ndof for req in trace) / max(steps, 1),
+                "d2h_bytes_per_step": 8 * sum(req.ndof for req in trace) / max(steps, 1)},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,7 +526,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c3", choices=["c3", "batched"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "batched", "served"])
+    ap.add_argument("--served-requests", type=int, default=32)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--batch-reps", type=int, default=3)
     args = ap.parse_args()
@@ -426,6 +537,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "served":
+        return run_served(args)
     return run_ours(args)
 
 

@@ -13,7 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfrforge_cuda.so")
 
 # status codes (frg_status)
-FRG_OK, FRG_DIVERGED, FRG_MAX_STEPS, FRG_RUNNING = 0, 1, 2, 3
+FRG_OK, FRG_DIVERGED, FRG_MAX_STEPS, FRG_RUNNING, FRG_CANCELLED = 0, 1, 2, 3, 4
 FRG_ERR_INVALID_ARG, FRG_ERR_UNSUPPORTED_HOOK, FRG_ERR_OOM = -1, -2, -3
 FRG_ERR_CUDA, FRG_ERR_TIMEOUT, FRG_ERR_STATE = -4, -5, -6
 
@@ -25,7 +25,7 @@ METHOD = {"null": 0, "persson": 1}
 AV_FORM = {"conservative_br0": 0, "element_local_DD": 1}
 GEOM = {"affine": 0, "wavy": 1, "metrics": 2}
 STATUS_SYMBOL = {FRG_OK: "ok", FRG_DIVERGED: "diverged", FRG_MAX_STEPS: "max_steps",
-                 FRG_RUNNING: "running"}
+                 FRG_RUNNING: "running", FRG_CANCELLED: "cancelled"}
 
 _dp = C.POINTER(C.c_double)
 
@@ -116,10 +116,20 @@ SIGNATURES = {
     "frg_batch_add": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(C.c_int)]),
     "frg_batch_remove": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_batch_get_solve": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "frg_batch_set_multirate": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_batch_start": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_int64]),
     "frg_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_result), C.POINTER(C.c_int)]),
     "frg_solve_bytes": (C.c_int, [C.POINTER(frg_solve_desc), C.POINTER(C.c_size_t)]),
+    "frg_server_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_int64, C.POINTER(C.c_void_p)]),
+    "frg_server_destroy": (C.c_int, [C.c_void_p]),
+    "frg_server_submit": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), _dp, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]),
+    "frg_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+    "frg_server_pump": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "frg_server_result": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(frg_result)]),
+    "frg_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int,
+                                            C.POINTER(C.c_int)]),
 }
 
 _lib = None

@@ -58,6 +58,11 @@ class Batch:
     def _chk(self, code, what):
         return L.check(code, self.ctx.handle, what)
 
+    def set_multirate(self, on: bool = True) -> None:
+        """Multirate scheduling: groups with cheaper steps take more steps per
+        round (results are unchanged; ``run``'s max_steps counts rounds)."""
+        self._chk(L.load().frg_batch_set_multirate(self.handle, 1 if on else 0), "frg_batch_set_multirate")
+
     def _solve(self, slot: int):
         s = C.c_void_p()
         self._chk(L.load().frg_batch_get_solve(self.handle, int(slot), C.byref(s)), "frg_batch_get_solve")

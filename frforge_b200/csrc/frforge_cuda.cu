@@ -536,6 +536,7 @@ const char* frg_status_string(int st) {
     case FRG_DIVERGED: return "diverged";
     case FRG_MAX_STEPS: return "max_steps";
     case FRG_RUNNING: return "running";
+    case FRG_CANCELLED: return "cancelled";
     case FRG_ERR_INVALID_ARG: return "invalid argument";
     case FRG_ERR_UNSUPPORTED_HOOK: return "unsupported hook";
     case FRG_ERR_OOM: return "out of device memory";

@@ -3,13 +3,19 @@
 //
 // Each instance is an ordinary frg_solve (its own state buffers, mesh arrays,
 // tables and status word).  Instances are grouped by (dim, NP, flux,
-// dissipation form, operator tables); every stage launches one kernel per
-// group over the ragged list of that group's tiles, so small instances fill
-// the GPU together instead of one after another.  A CUDA graph holds K steps
-// of [begin (all instances), stage kernels, end (all instances)]; instances
-// keep their own dt, time, step count and status, and finished instances
-// become no-ops.  Adding or removing an instance rebuilds the tile lists and
-// the graph at the next step boundary (continuous batching).
+// dissipation form, operator tables); a group advances as one chain of
+// [begin, stage 1..3, end] kernels over its members, the stage kernels
+// covering the ragged list of the members' tiles.  Groups are independent,
+// so each is a parallel branch of a CUDA graph (fork / join through events)
+// that holds several steps.  Instances keep their own dt, time, step count
+// and status; finished instances become no-ops.  Adding or removing an
+// instance rebuilds the lists and the graph at the next run (continuous
+// batching).
+//
+// Lockstep mode (default): every group takes the same number of steps per
+// run.  Multirate mode (frg_batch_set_multirate): a group whose step is
+// cheaper takes proportionally more steps per round, so cheap solves that need
+// many steps (long 1D meshes) are not held to the pace of heavy 2D ones.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -74,14 +80,18 @@ int batch_tile_shape(int dim, int np, int variant, int* tx, int* ty) {
   return -1;
 }
 
-// one thread per instance: the top / bottom of every instance's loop body
-__global__ void batch_begin_kernel(const BatchInst* insts, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && insts[i].sc) step_begin_device(insts[i].sc);
+// one thread per member of a group: the top / bottom of its loop body
+__global__ void batch_begin_kernel(const BatchInst* insts, const int* members, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const BatchInst& I = insts[members[k]];
+  if (I.sc) step_begin_device(I.sc);
 }
-__global__ void batch_end_kernel(const BatchInst* insts, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && insts[i].sc) step_end_device(insts[i].sc, insts[i].rk2 ? 2 : 3);
+__global__ void batch_end_kernel(const BatchInst* insts, const int* members, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const BatchInst& I = insts[members[k]];
+  if (I.sc) step_end_device(I.sc, I.rk2 ? 2 : 3);
 }
 // gather every instance's status for one host copy; count running ones
 __global__ void batch_status_kernel(const BatchInst* insts, int n, BatchStatus* out, int* nrun) {
@@ -118,23 +128,31 @@ struct frg_batch {
     int dim, np, flux, av, variant;
     HostOps ops;  // the group's tables (copied: members come and go)
     std::vector<BatchTile> tiles;
-    BatchTile* d_tiles = nullptr;
-    int d_cap = 0;
+    std::vector<int> members;
+    size_t ndof = 0;
+    int reps = 1;  // steps per round
+    void* d_buf = nullptr;  // tiles, then members
+    size_t d_bytes = 0;
+    const BatchTile* d_tiles() const { return (const BatchTile*)d_buf; }
+    const int* d_members() const { return (const int*)((const char*)d_buf + sizeof(BatchTile) * tiles.size()); }
   };
   std::vector<Group> groups;
-  // groups advance as parallel branches of each step: instance stages depend
-  // only on the same instance's previous stage
-  static constexpr int kAux = 8;
+  // groups advance as parallel branches: an instance's stages depend only on
+  // its own previous stage
+  static constexpr int kAux = 16;
   cudaStream_t aux[kAux] = {};
   cudaEvent_t fork = nullptr;
   cudaEvent_t join[kAux] = {};
   cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
+  int graph_rounds = 0;
   bool dirty = true;
+  bool multirate = false;
   size_t budget = 0, used = 0;  // HBM admission budget (bytes, 0 = none)
 };
 
 namespace {
+
+constexpr int kMaxReps = 32;  // multirate: most steps per round of one group
 
 int bcheck(frg_batch* b, cudaError_t e, const char* what) { return cuda_err(b->ctx, e, what); }
 
@@ -177,7 +195,11 @@ int rebuild(frg_batch* b) {
   int rc = bcheck(b, cudaMemcpyAsync(b->d_insts, insts.data(), sizeof(BatchInst) * b->cap,
                                      cudaMemcpyHostToDevice, b->ctx->stream), "batch instances");
   if (rc) return rc;
-  for (auto& g : b->groups) g.tiles.clear();
+  for (auto& g : b->groups) {
+    g.tiles.clear();
+    g.members.clear();
+    g.ndof = 0;
+  }
   for (int i = 0; i < b->cap; ++i) {
     frg_solve* s = b->slot[i];
     if (!s) continue;
@@ -210,26 +232,40 @@ int rebuild(frg_batch* b) {
     } else {
       for (int x = 0; x < s->nx; x += tx) grp->tiles.push_back(BatchTile{i, x, 0, 0});
     }
+    grp->members.push_back(i);
+    grp->ndof += s->ndof;
   }
-  // drop empty groups, upload tile lists
+  // drop empty groups, upload tile and member lists
   b->groups.erase(std::remove_if(b->groups.begin(), b->groups.end(),
                                  [](const frg_batch::Group& g) {
-                                   if (g.tiles.empty() && g.d_tiles) cudaFree(g.d_tiles);
-                                   return g.tiles.empty();
+                                   if (g.members.empty() && g.d_buf) cudaFree(g.d_buf);
+                                   return g.members.empty();
                                  }),
                   b->groups.end());
   for (auto& g : b->groups) {
-    if ((int)g.tiles.size() > g.d_cap) {
-      if (g.d_tiles) cudaFreeAsync(g.d_tiles, b->ctx->stream);
-      g.d_cap = (int)g.tiles.size() * 2;
-      if ((rc = bcheck(b, cudaMallocAsync((void**)&g.d_tiles, sizeof(BatchTile) * g.d_cap, b->ctx->stream),
-                       "tile list")))
-        return rc;
+    const size_t need = sizeof(BatchTile) * g.tiles.size() + sizeof(int) * g.members.size();
+    if (need > g.d_bytes) {
+      if (g.d_buf) cudaFree(g.d_buf);
+      g.d_buf = nullptr;
+      g.d_bytes = 0;
+      if ((rc = bcheck(b, cudaMalloc(&g.d_buf, 2 * need), "tile list"))) return rc;
+      g.d_bytes = 2 * need;
     }
-    if ((rc = bcheck(b, cudaMemcpyAsync(g.d_tiles, g.tiles.data(), sizeof(BatchTile) * g.tiles.size(),
-                                        cudaMemcpyHostToDevice, b->ctx->stream),
-                     "tile list upload")))
+    std::vector<char> host(need);
+    std::memcpy(host.data(), g.tiles.data(), sizeof(BatchTile) * g.tiles.size());
+    std::memcpy(host.data() + sizeof(BatchTile) * g.tiles.size(), g.members.data(),
+                sizeof(int) * g.members.size());
+    if ((rc = bcheck(b, cudaMemcpy(g.d_buf, host.data(), need, cudaMemcpyHostToDevice), "tile list upload")))
       return rc;
+  }
+  // steps per round: lockstep, or inversely proportional to the modelled
+  // step time of the group (a fixed launch floor plus a per-DOF cost)
+  double tmax = 0.0;
+  auto step_us = [](const frg_batch::Group& g) { return 25.0 + 3.0 * (double)g.ndof / 30e3; };
+  for (auto& g : b->groups) tmax = std::max(tmax, step_us(g));
+  for (auto& g : b->groups) {
+    g.reps = 1;
+    if (b->multirate) g.reps = std::max(1, std::min(kMaxReps, (int)(tmax / step_us(g))));
   }
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
@@ -239,48 +275,55 @@ int rebuild(frg_batch* b) {
   return FRG_OK;
 }
 
-int enqueue_group(frg_batch* b, const frg_batch::Group& g, cudaStream_t st) {
+int enqueue_group_step(frg_batch* b, const frg_batch::Group& g, cudaStream_t st) {
+  const int m = (int)g.members.size();
+  const int nb = (m + 127) / 128;
+  batch_begin_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
   for (int stage = 1; stage <= 3; ++stage) {
-    const int e = g.dim == 2 ? launch_batch2d(&g.ops, g.flux, g.av, g.variant, b->d_insts, g.d_tiles,
+    const int e = g.dim == 2 ? launch_batch2d(&g.ops, g.flux, g.av, g.variant, b->d_insts, g.d_tiles(),
                                               (int)g.tiles.size(), stage, kModeStage, st)
-                             : launch_batch1d(&g.ops, g.flux, g.av, b->d_insts, g.d_tiles,
+                             : launch_batch1d(&g.ops, g.flux, g.av, b->d_insts, g.d_tiles(),
                                               (int)g.tiles.size(), stage, kModeStage, st);
     if (e) return bcheck(b, (cudaError_t)e, "batched stage launch");
   }
-  return FRG_OK;
+  batch_end_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
+  return bcheck(b, cudaGetLastError(), "batch control kernels");
 }
 
-// One step of every instance: begin, the groups' three stages as parallel
-// branches (fork / join through events), end.
-int enqueue_batch_step(frg_batch* b) {
+// `rounds` rounds of every group (group g takes rounds * reps_g steps); the
+// groups are parallel branches forked from and joined back to the stream.
+int enqueue_rounds(frg_batch* b, int rounds) {
   cudaStream_t main = b->ctx->stream;
-  const int nb = (b->cap + 127) / 128;
-  batch_begin_kernel<<<nb, 128, 0, main>>>(b->d_insts, b->cap);
   const int ng = (int)b->groups.size();
   const int nbr = ng < frg_batch::kAux ? ng : frg_batch::kAux;
   int rc;
   if (nbr <= 1) {
-    for (auto& g : b->groups)
-      if ((rc = enqueue_group(b, g, main))) return rc;
-  } else {
-    if ((rc = bcheck(b, cudaEventRecord(b->fork, main), "fork"))) return rc;
-    for (int k = 0; k < nbr; ++k)
-      if ((rc = bcheck(b, cudaStreamWaitEvent(b->aux[k], b->fork, 0), "fork wait"))) return rc;
-    // largest groups first, dealt round-robin over the branches
-    std::vector<int> order(ng);
-    for (int k = 0; k < ng; ++k) order[k] = k;
-    std::sort(order.begin(), order.end(), [&](int x, int y) {
-      return b->groups[x].tiles.size() > b->groups[y].tiles.size();
-    });
-    for (int k = 0; k < ng; ++k)
-      if ((rc = enqueue_group(b, b->groups[order[k]], b->aux[k % nbr]))) return rc;
-    for (int k = 0; k < nbr; ++k) {
-      if ((rc = bcheck(b, cudaEventRecord(b->join[k], b->aux[k]), "join"))) return rc;
-      if ((rc = bcheck(b, cudaStreamWaitEvent(main, b->join[k], 0), "join wait"))) return rc;
-    }
+    for (int r = 0; r < rounds; ++r)
+      for (auto& g : b->groups)
+        for (int k = 0; k < g.reps; ++k)
+          if ((rc = enqueue_group_step(b, g, main))) return rc;
+    return FRG_OK;
   }
-  batch_end_kernel<<<nb, 128, 0, main>>>(b->d_insts, b->cap);
-  return bcheck(b, cudaGetLastError(), "batch control kernels");
+  if ((rc = bcheck(b, cudaEventRecord(b->fork, main), "fork"))) return rc;
+  for (int k = 0; k < nbr; ++k)
+    if ((rc = bcheck(b, cudaStreamWaitEvent(b->aux[k], b->fork, 0), "fork wait"))) return rc;
+  // heaviest groups first, dealt round-robin over the branches
+  std::vector<int> order(ng);
+  for (int k = 0; k < ng; ++k) order[k] = k;
+  std::sort(order.begin(), order.end(), [&](int x, int y) {
+    return b->groups[x].ndof * b->groups[x].reps > b->groups[y].ndof * b->groups[y].reps;
+  });
+  for (int r = 0; r < rounds; ++r)
+    for (int k = 0; k < ng; ++k) {
+      const frg_batch::Group& g = b->groups[order[k]];
+      for (int q = 0; q < g.reps; ++q)
+        if ((rc = enqueue_group_step(b, g, b->aux[k % nbr]))) return rc;
+    }
+  for (int k = 0; k < nbr; ++k) {
+    if ((rc = bcheck(b, cudaEventRecord(b->join[k], b->aux[k]), "join"))) return rc;
+    if ((rc = bcheck(b, cudaStreamWaitEvent(main, b->join[k], 0), "join wait"))) return rc;
+  }
+  return FRG_OK;
 }
 
 int poll(frg_batch* b, int* nrun) {
@@ -301,7 +344,7 @@ int poll(frg_batch* b, int* nrun) {
 
 void release_batch(frg_batch* b) {
   for (auto& g : b->groups)
-    if (g.d_tiles) cudaFree(g.d_tiles);
+    if (g.d_buf) cudaFree(g.d_buf);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (int k = 0; k < frg_batch::kAux; ++k) {
     if (b->aux[k]) cudaStreamDestroy(b->aux[k]);
@@ -423,6 +466,14 @@ int frg_solve_bytes(const frg_solve_desc* d, size_t* bytes) {
   return FRG_OK;
 }
 
+// Lockstep (0, default) or multirate (1) scheduling of the groups.
+int frg_batch_set_multirate(frg_batch* b, int on) {
+  if (!b) return FRG_ERR_INVALID_ARG;
+  b->multirate = on != 0;
+  b->dirty = true;
+  return FRG_OK;
+}
+
 int frg_batch_get_solve(frg_batch* b, int i, frg_solve** s) {
   if (!b || i < 0 || i >= b->cap || !s) return FRG_ERR_INVALID_ARG;
   *s = b->slot[i];
@@ -445,9 +496,10 @@ int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixe
   return FRG_OK;
 }
 
-// Advance every running instance by up to `max_steps` steps (or until all
-// have stopped).  results (capacity entries, may be NULL) receive each slot's
-// status; *n_running the number still running.
+// Advance every running instance by up to `max_steps` rounds (lockstep: one
+// step per round; multirate: reps_g steps per round for group g), or until
+// all have stopped.  results (capacity entries, may be NULL) receive each
+// slot's status; *n_running the number still running.
 int frg_batch_run(frg_batch* b, int64_t max_steps, frg_result* results, int* n_running) {
   if (!b || max_steps < 1) return FRG_ERR_INVALID_ARG;
   cudaSetDevice(b->ctx->device);
@@ -456,35 +508,37 @@ int frg_batch_run(frg_batch* b, int64_t max_steps, frg_result* results, int* n_r
   int64_t total = 0;
   int nrun = 0;
   for (int i = 0; i < b->cap; ++i) nrun += b->running[i] ? 1 : 0;
-  // steps per graph: a few milliseconds of work per launch
-  size_t ndof = 0;
-  for (frg_solve* s : b->slot)
-    if (s) ndof += s->ndof;
-  const int K = ndof > 4000000 ? 4 : (ndof > 400000 ? 8 : 16);
+  // rounds per graph: a few milliseconds of work and at most ~600 kernels
+  size_t work = 0;
+  int nodes = 0;
+  for (auto& g : b->groups) {
+    work += g.ndof * (size_t)g.reps;
+    nodes += 5 * g.reps;
+  }
+  int K = work > 4000000 ? 4 : (work > 400000 ? 8 : 16);
+  while (K > 1 && K * nodes > 600) K /= 2;
   while (nrun > 0 && total < max_steps) {
     const int k = (int)std::min<int64_t>(K, max_steps - total);
     if (k == K) {
-      if (!b->graph || b->graph_steps != K) {
+      if (!b->graph || b->graph_rounds != K) {
         if (b->graph) cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
         cudaGraph_t g;
         if ((rc = bcheck(b, cudaStreamBeginCapture(b->ctx->stream, cudaStreamCaptureModeThreadLocal),
                          "batch capture")))
           return rc;
-        int crc = FRG_OK;
-        for (int s = 0; s < K && !crc; ++s) crc = enqueue_batch_step(b);
+        const int crc = enqueue_rounds(b, K);
         cudaError_t ce = cudaStreamEndCapture(b->ctx->stream, &g);
         if (crc) return crc;
         if ((rc = bcheck(b, ce, "batch capture end"))) return rc;
         ce = cudaGraphInstantiate(&b->graph, g, 0);
         cudaGraphDestroy(g);
         if ((rc = bcheck(b, ce, "batch graph"))) return rc;
-        b->graph_steps = K;
+        b->graph_rounds = K;
       }
       if ((rc = bcheck(b, cudaGraphLaunch(b->graph, b->ctx->stream), "batch graph launch"))) return rc;
-    } else {
-      for (int s = 0; s < k; ++s)
-        if ((rc = enqueue_batch_step(b))) return rc;
+    } else if ((rc = enqueue_rounds(b, k))) {
+      return rc;
     }
     total += k;
     if ((rc = poll(b, &nrun))) return rc;

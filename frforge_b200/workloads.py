@@ -139,3 +139,90 @@ def c4_instances(seed: int = DEFAULT_SEED, count: int = 64, steps: int = 200) ->
         out.append(Workload2D("c2" if periodic else "c3", n, p, flux, "persson_av", c_av, periodic, 0.1,
                               steps, seed=seed + 1 + i))
     return out
+
+
+@dataclass
+class Request:
+    """One served solve of the served trace."""
+    arrival: float  # seconds after the trace start
+    dim: int
+    n: int  # elements per side (2D) or elements (1D)
+    p: int
+    flux: str
+    periodic: bool  # density wave (True) or Riemann problem (False); periodic domain
+    wavy: bool  # 2D: sinusoidal mesh warp, amplitude 0.05, analytic metrics
+    t_final: float
+    seed: int
+    cfl: float = 0.1
+
+    @property
+    def ndof(self) -> int:
+        return self.n * self.n * (self.p + 1) ** 2 * 4 if self.dim == 2 else self.n * (self.p + 1) * 3
+
+    def build(self, F):
+        """(state, eq, method) for the frforge_b200 module F, IC filled in."""
+        g = splitmix64(self.seed)
+        ops = F.build_operators(self.p)
+        method = F.PerssonAVMethod(c_av=0.1)
+        bc = F.PeriodicBC
+        if self.dim == 1:
+            mesh = F.Mesh1D(0.0, 1.0, self.n, bc(), bc())
+            st = F.allocate_state(mesh, ops, 3, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+            X = mesh.physical_coords(ops)
+            if self.periodic:
+                phi = uniform(g, 0.0, 2 * math.pi)
+                r, u, p = 1.0 + 0.2 * np.sin(2 * math.pi * X + phi), 1.0 + 0 * X, 1.0 + 0 * X
+            else:
+                L, R = two_state_1d(self.seed)
+                m = [(a + b) / 2.0 for a, b in zip(L, R)]
+                L = [mm + 0.25 * (a - mm) for mm, a in zip(m, L)]
+                R = [mm + 0.25 * (b - mm) for mm, b in zip(m, R)]
+                r = np.where(X < 0.5, L[0], R[0])
+                u = np.where(X < 0.5, L[1], R[1])
+                p = np.where(X < 0.5, L[2], R[2])
+            st.u[...] = np.stack([r, r * u, p / 0.4 + 0.5 * r * u * u], axis=-1)
+            return st, F.Euler1D(1.4), method
+        if self.wavy:
+            mesh = F.make_wavy_mesh2d(self.n, self.n, amp=0.05, left_bc=bc(), right_bc=bc(), bottom_bc=bc(),
+                                      top_bc=bc())
+        else:
+            mesh = F.Mesh2D(0.0, 1.0, 0.0, 1.0, self.n, self.n, bc(), bc(), bc(), bc())
+        st = F.allocate_state(mesh, ops, 4, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+        X, Y = mesh.physical_coords(ops)
+        w = Workload2D("c2" if self.periodic else "c3", self.n, self.p, self.flux, "persson_av", 0.1,
+                       self.periodic, self.cfl, 0, seed=self.seed)
+        st.u[...] = w.initial_state(X, Y)
+        return st, F.Euler2D(1.4), method
+
+
+def served_trace(seed: int = DEFAULT_SEED, count: int = 32, rate: float = 200.0, n2d=(16, 384),
+                 n1d=(128, 4096), t_final=(0.05, 0.25)) -> List[Request]:
+    """The served workload: ``count`` requests with Poisson arrivals at
+    ``rate`` per second, drawn from one SplitMix64 stream, per request in this
+    order: inter-arrival Exp(rate), 1D or 2D with probability 1/2, size (2D
+    n ~ U{n2d}, 1D Ne ~ U{n1d}), P ~ U{1..5}, flux HLLC or Rusanov, density
+    wave or Riemann problem, for 2D a wavy mesh (amplitude 0.05) with
+    probability 1/4, t_final ~ U[t_final].  Persson AV (BR0, c_av 0.1),
+    SSP-RK3, CFL 0.1, periodic domains.  Riemann states are drawn as for the
+    single-solve workloads and their jumps about the mean scaled by 0.25
+    (unscaled, the scheme without a limiter loses positivity); 2D Riemann
+    problems use the four-quadrant rule.  Domains are periodic because the
+    transmissive boundary of the reference scheme has a growing mode at high
+    P (a 1e-12 perturbation at the right boundary of a P=5 Rusanov mesh grows
+    to 5e-4 in 2000 steps in the oracle), so whether a long transmissive run
+    diverges depends on rounding noise."""
+    g = splitmix64(seed)
+    t = 0.0
+    out = []
+    for i in range(count):
+        t += -math.log(1.0 - next(g)) / rate
+        dim = 2 if next(g) < 0.5 else 1
+        lo, hi = n2d if dim == 2 else n1d
+        n = lo + min(int((hi - lo + 1) * next(g)), hi - lo)
+        p = 1 + min(int(5.0 * next(g)), 4)
+        flux = "hllc" if next(g) < 0.5 else "rusanov"
+        periodic = next(g) < 0.5
+        wavy = dim == 2 and next(g) < 0.25
+        tf = uniform(g, t_final[0], t_final[1])
+        out.append(Request(t, dim, n, p, flux, periodic, wavy, tf, seed + 1000 + i))
+    return out

@@ -39,6 +39,7 @@ typedef enum {
   FRG_DIVERGED = 1,
   FRG_MAX_STEPS = 2,
   FRG_RUNNING = 3,               /* batched instance still advancing */
+  FRG_CANCELLED = 4,             /* served request cancelled */
   FRG_ERR_INVALID_ARG = -1,      /* ArgumentError in the reference */
   FRG_ERR_UNSUPPORTED_HOOK = -2, /* a capturing hook with no GPU implementation */
   FRG_ERR_OOM = -3,              /* device allocation / admission budget */
@@ -148,6 +149,7 @@ typedef struct {
 typedef struct frg_ctx frg_ctx;
 typedef struct frg_solve frg_solve;
 typedef struct frg_batch frg_batch;
+typedef struct frg_server frg_server;
 
 /* ---- library / context ---------------------------------------------- */
 int frg_abi_version(void);
@@ -258,6 +260,11 @@ int frg_batch_destroy(frg_batch* b); /* destroys its instances too */
    frg_batch_start. */
 int frg_batch_add(frg_batch* b, const frg_solve_desc* desc, int* slot);
 int frg_batch_remove(frg_batch* b, int slot);
+/* Scheduling: lockstep (0, default: every instance takes one step per round)
+   or multirate (1: a group of instances whose step is cheaper takes up to 32
+   steps per round, so cheap solves that need many steps keep pace).  Results
+   do not depend on the mode; max_steps of frg_batch_run counts rounds. */
+int frg_batch_set_multirate(frg_batch* b, int on);
 /* The instance's solve: frg_upload_state / frg_download_state /
    frg_residual work on it while it is not running. */
 int frg_batch_get_solve(frg_batch* b, int slot, frg_solve** s);
@@ -272,6 +279,34 @@ int frg_batch_run(frg_batch* b, int64_t max_steps, frg_result* results, int* n_r
 /* Upper bound of the device bytes a solve of this descriptor holds (the
    admission test of a served batch). */
 int frg_solve_bytes(const frg_solve_desc* desc, size_t* bytes);
+
+/* ----------------------------------------------------------------- server
+   A request queue in front of a batch (no counterpart in the reference,
+   whose case runners, src/cli/run.jl:267, solve one request at a time).
+   frg_server_pump admits queued requests in arrival order into free slots
+   while their footprint fits the HBM budget, advances the batch by up to
+   steps_per_pump rounds (multirate) and delivers finished requests (final
+   state copied to u_out, slot freed and refilled at once).  The caller's loop
+   drives the server; there is no internal thread. */
+int frg_server_create(frg_ctx* ctx, int slots, size_t hbm_budget, int64_t steps_per_pump,
+                      frg_server** out);
+int frg_server_destroy(frg_server* s);
+/* Queue one solve.  desc and every array it points to, u0 (ndof doubles,
+   host) and u_out (ndof doubles, host, written on completion) must stay
+   valid until the request completes.  FRG_ERR_OOM if the request alone
+   exceeds the budget. */
+int frg_server_submit(frg_server* s, const frg_solve_desc* desc, const double* u0, double t0,
+                      double t_final, double cfl, double fixed_dt, int64_t max_steps,
+                      double* u_out, int64_t* request_id);
+/* Cancel a queued or running request (result FRG_CANCELLED). */
+int frg_server_cancel(frg_server* s, int64_t request_id);
+/* One scheduling round; counts of requests completed by this call, still
+   queued and running. */
+int frg_server_pump(frg_server* s, int* n_done, int* n_queued, int* n_active);
+/* *done = 1 once the request completed; r = its status, steps and time. */
+int frg_server_result(frg_server* s, int64_t request_id, int* done, frg_result* r);
+/* Up to cap request ids completed since the last call, in completion order. */
+int frg_server_take_completed(frg_server* s, int64_t* ids, int cap, int* n);
 
 #ifdef __cplusplus
 }
