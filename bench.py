@@ -8,6 +8,7 @@ evaluations over all 512^2 x 16 x 4 = 16.8M degrees of freedom.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --workload batched     # 64 mixed solves, batched vs one at a time
   python bench.py --workload served      # Poisson request trace, served vs one at a time
+  python bench.py --ncu-target [--n 256] # a few stage launches of the workload, for ncu
 
 ours: value = DOF-stage/s with the state resident in HBM, timed with CUDA
 events on the library's stream (max over ranks); e2e = the same metric through
@@ -519,6 +520,25 @@ def run_served(args):
     return 0
 
 
+def run_ncu_target(args):
+    """A short, fixed launch sequence for ncu captures: the 512^2 workload
+    (or --n elements per side, same P, flux, method, IC), default tile
+    variant, one prime launch then --steps SSP-RK3 steps with direct
+    launches (begin, stage 1, 2, 3, end per step)."""
+    import frforge_b200 as F
+    from frforge_b200.workloads import C3, Workload2D
+
+    w = Workload2D(C3.name, args.n, C3.p, C3.flux, C3.method, C3.c_av, C3.periodic, C3.cfl, C3.steps,
+                   seed=C3.seed, jump_scale=C3.jump_scale)
+    st, method = w.build(F)
+    solve = F.GpuSolve(st, F.Euler2D(1.4), method)
+    solve.upload(st.u, 0.0)
+    ms, r = solve.time_stages(args.steps, cfl=C3.cfl)
+    print(json.dumps({"ncu_target": True, "n": args.n, "steps": args.steps, "stage_ms": [float(x) for x in ms],
+                      "status": r["status"]}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -528,6 +548,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="c3", choices=["c3", "batched", "served"])
     ap.add_argument("--served-requests", type=int, default=32)
+    ap.add_argument("--ncu-target", action="store_true")
+    ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--batch-reps", type=int, default=3)
     args = ap.parse_args()
@@ -535,6 +557,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.ncu_target:
+        return run_ncu_target(args)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "served":

@@ -205,7 +205,7 @@ int rebuild(frg_batch* b) {
     if (!s) continue;
     const int av = s->dim == 2 ? s->L2.av : s->L1.av;
     const int flux = s->dim == 2 ? s->L2.flux : s->L1.flux;
-    const int variant = s->dim == 2 ? s->L2.variant : 0;
+    const int variant = 0;  // the batched kernels use one fixed tile shape per NP
     frg_batch::Group* grp = nullptr;
     for (auto& g : b->groups)
       if (g.dim == s->dim && g.np == s->np && g.flux == flux && g.av == av && g.variant == variant &&

@@ -35,45 +35,53 @@ OpsT<NP> make_ops(const HostOps& h) {
 // Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory).
 // Variant 0 is the default, the fastest measured on a B200 for large meshes
 // (P=3: 512^2, P=4/5: 384^2); the autotuner times all of them on the solve.
+// The batched kernels use variant `batch`.
 template <int NP>
 struct Variants2D;
+#define FRG_V(NPv, idx, tx, ty, minb, u0s)                                              \
+  template <>                                                                             \
+  struct Variants2D<NPv>::V_<idx> {                                                       \
+    static constexpr int TX = tx, TY = ty, MINB = minb;                                   \
+    static constexpr bool U0S = u0s;                                                      \
+  };
 template <>
 struct Variants2D<2> {
-  static constexpr int n = 2;
+  static constexpr int n = 2, batch = 1;
   template <int V> struct V_;
 };
-template <> struct Variants2D<2>::V_<0> { static constexpr int TX = 8, TY = 8, MINB = 2; static constexpr bool U0S = true; };
-template <> struct Variants2D<2>::V_<1> { static constexpr int TX = 8, TY = 4, MINB = 3; static constexpr bool U0S = false; };
+FRG_V(2, 0, 8, 8, 2, true)
+FRG_V(2, 1, 8, 4, 3, false)
 template <>
 struct Variants2D<3> {
-  static constexpr int n = 3;
+  static constexpr int n = 3, batch = 0;
   template <int V> struct V_;
 };
-template <> struct Variants2D<3>::V_<0> { static constexpr int TX = 8, TY = 6, MINB = 2; static constexpr bool U0S = true; };
-template <> struct Variants2D<3>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> struct Variants2D<3>::V_<2> { static constexpr int TX = 4, TY = 4, MINB = 4; static constexpr bool U0S = false; };
+FRG_V(3, 0, 8, 6, 2, true)
+FRG_V(3, 1, 8, 3, 3, false)
+FRG_V(3, 2, 4, 4, 4, false)
 template <>
 struct Variants2D<4> {
-  static constexpr int n = 3;
+  static constexpr int n = 3, batch = 0;
   template <int V> struct V_;
 };
-template <> struct Variants2D<4>::V_<0> { static constexpr int TX = 8, TY = 2, MINB = 4; static constexpr bool U0S = false; };
-template <> struct Variants2D<4>::V_<1> { static constexpr int TX = 8, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> struct Variants2D<4>::V_<2> { static constexpr int TX = 8, TY = 4, MINB = 2; static constexpr bool U0S = true; };
+FRG_V(4, 0, 8, 2, 4, false)
+FRG_V(4, 1, 8, 3, 3, false)
+FRG_V(4, 2, 8, 4, 2, true)
 template <>
 struct Variants2D<5> {
-  static constexpr int n = 2;
+  static constexpr int n = 2, batch = 0;
   template <int V> struct V_;
 };
-template <> struct Variants2D<5>::V_<0> { static constexpr int TX = 4, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> struct Variants2D<5>::V_<1> { static constexpr int TX = 4, TY = 4, MINB = 2; static constexpr bool U0S = true; };
+FRG_V(5, 0, 4, 3, 3, false)
+FRG_V(5, 1, 4, 4, 2, true)
 template <>
 struct Variants2D<6> {
-  static constexpr int n = 2;
+  static constexpr int n = 2, batch = 0;
   template <int V> struct V_;
 };
-template <> struct Variants2D<6>::V_<0> { static constexpr int TX = 3, TY = 3, MINB = 3; static constexpr bool U0S = false; };
-template <> struct Variants2D<6>::V_<1> { static constexpr int TX = 4, TY = 3, MINB = 2; static constexpr bool U0S = true; };
+FRG_V(6, 0, 3, 3, 3, false)
+FRG_V(6, 1, 4, 3, 2, true)
+#undef FRG_V
 
 template <int NP, int FLUX, int AV, int V>
 int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
@@ -171,20 +179,9 @@ int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles
 }
 
 template <int NP, int FLUX, int AV>
-int batch2d_inst(const HostOps& h, int variant, const BatchInst* insts, const BatchTile* tiles, int ntiles,
+int batch2d_inst(const HostOps& h, int /*variant*/, const BatchInst* insts, const BatchTile* tiles, int ntiles,
                  int stage, int mode, cudaStream_t st) {
-  const int v = (variant >= 0 && variant < Variants2D<NP>::n) ? variant : 0;
-  switch (v) {
-    case 1:
-      if constexpr (Variants2D<NP>::n > 1) return batch2d_var<NP, FLUX, AV, 1>(h, insts, tiles, ntiles, stage, mode, st);
-      break;
-    case 2:
-      if constexpr (Variants2D<NP>::n > 2) return batch2d_var<NP, FLUX, AV, 2>(h, insts, tiles, ntiles, stage, mode, st);
-      break;
-    default:
-      break;
-  }
-  return batch2d_var<NP, FLUX, AV, 0>(h, insts, tiles, ntiles, stage, mode, st);
+  return batch2d_var<NP, FLUX, AV, Variants2D<NP>::batch>(h, insts, tiles, ntiles, stage, mode, st);
 }
 
 template <int NP>
@@ -237,33 +234,15 @@ int batch1d_np(const HostOps& h, int flux, int av, const BatchInst* insts, const
 }
 
 template <int NP>
-int tile_shape_np(int dim, int variant, int* tx, int* ty) {
+int tile_shape_np(int dim, int /*variant*/, int* tx, int* ty) {
   if (dim == 1) {
     *tx = Tile1D<NP>::TX;
     *ty = 1;
     return 0;
   }
-  const int v = (variant >= 0 && variant < Variants2D<NP>::n) ? variant : 0;
-  switch (v) {
-    case 1:
-      if constexpr (Variants2D<NP>::n > 1) {
-        *tx = Variants2D<NP>::template V_<1>::TX;
-        *ty = Variants2D<NP>::template V_<1>::TY;
-        return 0;
-      }
-      break;
-    case 2:
-      if constexpr (Variants2D<NP>::n > 2) {
-        *tx = Variants2D<NP>::template V_<2>::TX;
-        *ty = Variants2D<NP>::template V_<2>::TY;
-        return 0;
-      }
-      break;
-    default:
-      break;
-  }
-  *tx = Variants2D<NP>::template V_<0>::TX;
-  *ty = Variants2D<NP>::template V_<0>::TY;
+  using VB = typename Variants2D<NP>::template V_<Variants2D<NP>::batch>;
+  *tx = VB::TX;
+  *ty = VB::TY;
   return 0;
 }
 

@@ -1,10 +1,10 @@
 // Fused 2D FR stage kernel for sm_100a (FP64).
 //
-// One CTA owns a TX x TY tile of elements and stages the tile plus a
+// A CTA owns a TX x TY tile of elements and stages the tile plus a
 // one-element halo ring (no corners) of the stage input in shared memory.
 // Everything a stage needs happens on chip:
-//   P0  cp.async prefetch of u_s (tile + halo) and, as a second commit group
-//       that lands while P1-P4 compute, the step-start state u0 of the tile
+//   P0  cp.async copies of the tile: u_s (tile + halo), the step-start state
+//       u0 of the tile and the per-slot mesh values (eps, Jx, Jy, dx, dy)
 //   P1  physical fluxes -> contravariant F~, G~ at every own solution point
 //       (Residual2D.jl:342-352)
 //   P2  every face point of the tile once: u traces of both sides
@@ -19,9 +19,15 @@
 //   P6  sensor of the NEW state (sense!, PerssonAV2D.jl:20-59), element
 //       viscosity eps for the next stage (element_viscosities_2d,
 //       PerssonAV2D.jl:89-109) and the CFL wave speed (compute_dt,
-//       SSP_RK3.jl:126-133) as one atomic max per CTA.
+//       SSP_RK3.jl:126-133) as one atomic max per tile.
 // Halo values come from the neighbouring tiles' own loads, so they are
 // L2 hits; DRAM traffic per stage is the algorithmic u_s + u0 + u_out.
+//
+// The single-solve kernel and the batched kernels run one tile per CTA
+// through the same phases (tile_slots / tile_issue / tile_compute).  A
+// persistent variant that copied each CTA's next tile into a second buffer
+// while computing the current one measured slower on a B200: with four
+// resident CTAs per SM the other CTAs already cover the load latency.
 //
 // Shared-memory blocks use odd strides (in doubles) between elements and
 // lanes walk over elements first, so a warp's 8-byte accesses spread over
@@ -34,8 +40,8 @@ namespace frg {
 
 template <int NP>
 struct Tile2D;
-// Tile shapes (elements): two CTAs of 256 threads reside per SM (register
-// bound at 128/thread), so each tile's shared memory stays under ~113 KB.
+// Default tile shapes (elements) of stage2d_kernel<..> without explicit
+// tile arguments.
 template <>
 struct Tile2D<2> {
   static constexpr int TX = 8, TY = 8;
@@ -59,8 +65,8 @@ struct Tile2D<6> {
 
 constexpr int odd_up(int n) { return (n % 2) ? n : n + 1; }
 
-// U0S: stage the step-start state u0 in shared memory (prefetched under the
-// compute); otherwise the epilogue reads it from global memory.
+// Shared-memory layout.  U0S: stage the step-start state u0 in shared memory
+// (copied with the tile); otherwise the epilogue reads it from global memory.
 template <int NP, int TX, int TY, bool U0S = true, int MINB = 2>
 struct Smem2D {
   static constexpr int NEQ = 4, NP2 = NP * NP;
@@ -68,20 +74,26 @@ struct Smem2D {
   static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
   static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
   static constexpr int FS = odd_up(NP * 8);     // face stride: NP points x (fhat[4], ghat[4])
-  // doubles
-  static constexpr int oU = 0;                      // [NSLOT][ES]
-  static constexpr int oF = oU + NSLOT * ES;        // [NOWN][ES]
+  // one tile buffer (doubles): u_s of tile + halo, u0 of the tile, per-slot
+  // raw mesh values [5][NSLOT] = eps, Jx, Jy, dx, dy
+  static constexpr int bU = 0;
+  static constexpr int bU0 = bU + NSLOT * ES;
+  static constexpr int bRaw = bU0 + (U0S ? NOWN * ES : 0);
+  static constexpr int bDoubles = bRaw + 5 * NSLOT;
+  static constexpr int oF = bDoubles;               // [NOWN][ES]
   static constexpr int oG = oF + NOWN * ES;         // [NOWN][ES]
-  static constexpr int oU0 = oG + NOWN * ES;        // [NOWN][ES] u0 prefetch
-  static constexpr int oFV = oU0 + (U0S ? NOWN * ES : 0);  // [NFV][FS]
+  static constexpr int oFV = oG + NOWN * ES;        // [NFV][FS]
   static constexpr int oFH = oFV + NFV * FS;        // [NFH][FS]
-  static constexpr int oSlot = oFH + NFH * FS;      // per slot: eps, Jx, Jy, dx, dy
-  static constexpr int oRed = oSlot + NSLOT * 5;    // reduction scratch
+  // per-slot factors of P2-P4: 1/(Jx Jy), eps/Jx^2, eps/Jy^2, 1/Jx, 1/Jy,
+  // eps/Jx, eps/Jy
+  static constexpr int oDer = oFH + NFH * FS;       // [7][NSLOT]
+  static constexpr int oRed = oDer + 7 * NSLOT;     // reduction scratch
   static constexpr int nDoubles = oRed + 32;
-  static constexpr int nInts = NSLOT * 2 + 8;
+  static constexpr int nInts = NSLOT * 2 + 8;  // element ids, flags
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
   // 1 KB reserved per CTA plus the batched kernels' static descriptors
-  static_assert(MINB * (bytes + 1024 + kBatchStaticSmem) <= 228 * 1024, "MINB CTAs must fit in one SM's shared memory");
+  static_assert(MINB * (bytes + 1024 + kBatchStaticSmem) <= 228 * 1024,
+                "MINB CTAs must fit in one SM's shared memory");
 };
 
 constexpr int kStageThreads = 256;
@@ -99,58 +111,57 @@ FRG_DEV void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// One tile of one stage.  TX x TY: tile (elements); MINB: CTAs per SM the
-// register budget targets (only sizes the static shared-memory check);
-// U0S: u0 staged in shared memory.  tx0, ty0: first element of the tile.
-template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S>
-__device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
-                                             const StageBufs& B, const int tx0, const int ty0) {
-  using S = Smem2D<NP, TX, TY, U0S, MINB>;
-  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
-  constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, NOWN = S::NOWN;
-  constexpr int NFV = S::NFV, NFH = S::NFH;
-  constexpr int NT = kStageThreads;
-  constexpr bool kBR0 = (AV == kAvBR0);
-  constexpr bool kAV = (AV != kAvNone);
+// One tile buffer in shared memory.
+struct TileBuf {
+  double* U;    // [NSLOT][ES]
+  double* U0;   // [NOWN][ES]
+  double* raw;  // [5][NSLOT]
+  int* el;      // [NSLOT]
+  int* flag;    // [NSLOT]
+};
 
-  extern __shared__ __align__(16) double smem[];
-  double* sU = smem + S::oU;
-  double* sF = smem + S::oF;
-  double* sG = smem + S::oG;
-  double* sU0 = smem + S::oU0;
-  double* sFV = smem + S::oFV;
-  double* sFH = smem + S::oFH;
-  double* sEps = smem + S::oSlot;
-  double* sJx = sEps + NSLOT;
-  double* sJy = sJx + NSLOT;
-  double* sDx = sJy + NSLOT;
-  double* sDy = sDx + NSLOT;
-  double* sRed = smem + S::oRed;
-  int* sEl = reinterpret_cast<int*>(smem + S::nDoubles);
-  int* sFlag = sEl + NSLOT;
+template <class S>
+FRG_DEV TileBuf tile_buf(double* smem) {
+  TileBuf t;
+  t.U = smem + S::bU;
+  t.U0 = smem + S::bU0;
+  t.raw = smem + S::bRaw;
+  t.el = reinterpret_cast<int*>(smem + S::nDoubles);
+  t.flag = t.el + S::NSLOT;
+  return t;
+}
 
-  const int tid = threadIdx.x;
-  const int nx = M.nx, ny = M.ny;
-  const size_t cs = (size_t)M.nel * NP2;  // component stride
+// Stage-wide control values, the same for every tile of the launch.
+struct StageCtl {
+  double dt, tstage;
+  bool prime, need_u0;
+};
 
-  double dt = 0.0, tstage = 0.0;
+// false: the stage is skipped (the step is inactive or an earlier stage
+// flagged a non-finite value).
+FRG_DEV bool stage_control(const StageBufs& B, StageCtl& c) {
+  c.dt = 0.0;
+  c.tstage = 0.0;
   if (B.use_sc) {
-    if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
-    dt = B.sc->dt;
+    if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return false;
+    c.dt = B.sc->dt;
     const double t0 = B.sc->t0;
-    tstage = (B.stage == 1) ? t0 : (B.stage == 2 ? t0 + dt : t0 + dt / 2.0);
+    c.tstage = (B.stage == 1) ? t0 : (B.stage == 2 ? t0 + c.dt : t0 + c.dt / 2.0);
   } else if (B.sc) {
-    tstage = B.sc->t;
-    dt = B.sc->dt;
+    c.tstage = B.sc->t;
+    c.dt = B.sc->dt;
   }
-  const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
-  const bool need_u0 = (B.mode == kModeStage) && (B.stage != 1);
+  c.prime = (B.mode == kModePrime) || (B.mode == kModeSense);
+  c.need_u0 = (B.mode == kModeStage) && (B.stage != 1);
+  return true;
+}
 
-
-  // ---------------------------------------------------------------- slots
-  // element ids first (integer work only), so the tile copies can be issued
-  // before any metadata load
-  for (int s = tid; s < NSLOT; s += NT) {
+// Slots of a tile: element id (-1: none) and flags of every tile + halo slot.
+template <class S>
+FRG_DEV void tile_slots(const Mesh2Dev& M, const TileBuf& tb, const int tx0, const int ty0, const bool prime) {
+  constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, TX = S::BX - 2, TY = S::BY - 2;
+  const int nx = M.nx, ny = M.ny;
+  for (int s = threadIdx.x; s < NSLOT; s += kStageThreads) {
     const int bx = s % BX, by = s / BX;
     const bool corner = (bx == 0 || bx == BX - 1) && (by == 0 || by == BY - 1);
     int gx = tx0 + bx - 1, gy = ty0 + by - 1;
@@ -175,53 +186,123 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
         if (prime && !(fl & kSlotOwn)) el = -1;  // prime/sense: own elements only
       }
     }
-    sEl[s] = el;
-    sFlag[s] = fl;
+    tb.el[s] = el;
+    tb.flag[s] = fl;
   }
-  __syncthreads();
+}
 
-  // ----------------------------------------------- P0 async prefetch
-  {
-    // u_s of tile + halo: rows of slots are contiguous in global memory per
-    // component, so consecutive threads copy consecutive doubles
-    constexpr int ROW = BX * NP2;
-    constexpr int TOTAL = BY * NEQ * ROW;
-    for (int idx = tid; idx < TOTAL; idx += NT) {
-      const int r = idx % ROW, t = idx / ROW;
-      const int c = t % NEQ, by = t / NEQ;
-      const int bx = r / NP2, k = r % NP2;
-      const int s = by * BX + bx;
-      const int el = sEl[s];
-      if (el >= 0) cp_async8(&sU[s * ES + c * NP2 + k], &B.us[c * cs + (size_t)el * NP2 + k]);
+// P0: issue the cp.async copies of a tile (one commit group); the slots of
+// the buffer must be visible to every thread.
+template <int NP, int AV, class S>
+FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb, const StageCtl& c) {
+  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, BX = S::BX, BY = S::BY, NSLOT = S::NSLOT;
+  constexpr int TX = BX - 2, TY = BY - 2;
+  constexpr int NT = kStageThreads;
+  constexpr bool U0S = (S::bRaw != S::bU0);
+  const int tid = threadIdx.x;
+  const size_t cs = (size_t)M.nel * NP2;  // component stride
+  // Thread (e, k): solution point k of every EL-th slot, all components.
+  // Per copy only the two addresses advance; a warp covers whole elements,
+  // which are contiguous per component in global memory.
+  constexpr int EL = NT / NP2;
+  const int k = tid % NP2, e = tid / NP2;
+  if (e < EL) {
+    for (int s = e; s < NSLOT; s += EL) {
+      const int el = tb.el[s];
+      if (el < 0) continue;
+      double* dst = tb.U + s * ES + k;
+      const double* src = B.us + (size_t)el * NP2 + k;
+#pragma unroll
+      for (int cc = 0; cc < NEQ; ++cc) cp_async8(dst + cc * NP2, src + cc * cs);
     }
-    cp_async_commit();
-    if (U0S && need_u0) {
-      constexpr int OROW = TX * NP2;
-      constexpr int OTOTAL = TY * NEQ * OROW;
-      for (int idx = tid; idx < OTOTAL; idx += NT) {
-        const int r = idx % OROW, t = idx / OROW;
-        const int c = t % NEQ, oy = t / NEQ;
-        const int ox = r / NP2, k = r % NP2;
-        const int s = (oy + 1) * BX + ox + 1;
-        if (sFlag[s] & kSlotOwn)
-          cp_async8(&sU0[(oy * TX + ox) * ES + c * NP2 + k], &B.u0[c * cs + (size_t)sEl[s] * NP2 + k]);
+    if (U0S && c.need_u0) {
+      for (int o = e; o < TX * TY; o += EL) {
+        const int s = (o / TX + 1) * BX + (o % TX) + 1;
+        if (!(tb.flag[s] & kSlotOwn)) continue;
+        double* dst = tb.U0 + o * ES + k;
+        const double* src = B.u0 + (size_t)tb.el[s] * NP2 + k;
+#pragma unroll
+        for (int cc = 0; cc < NEQ; ++cc) cp_async8(dst + cc * NP2, src + cc * cs);
       }
     }
-    cp_async_commit();
   }
-  // slot metadata while the copies are in flight
+  // per-slot mesh values
+  for (int s = tid; s < NSLOT; s += NT) {
+    const int el = tb.el[s];
+    if (el < 0) continue;
+    const int gx = el % M.nx, gy = el / M.nx;
+    if (AV != kAvNone && !c.prime) cp_async8(&tb.raw[s], &B.eps_in[el]);
+    cp_async8(&tb.raw[NSLOT + s], &M.Jx[gx]);
+    cp_async8(&tb.raw[2 * NSLOT + s], &M.Jy[gy]);
+    cp_async8(&tb.raw[3 * NSLOT + s], &M.dx[gx]);
+    cp_async8(&tb.raw[4 * NSLOT + s], &M.dy[gy]);
+  }
+  cp_async_commit();
+}
+
+// P1-P6 of one tile whose copies are in tb.  WAIT: cp.async groups that may
+// still be pending when the tile starts.
+template <int NP, int FLUX, int AV, class S, int WAIT>
+FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P, const StageBufs& B,
+                          const TileBuf& tb, double* smem, const StageCtl& ctl) {
+  constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
+  constexpr int BX = S::BX, NSLOT = S::NSLOT, NOWN = S::NOWN;
+  constexpr int TX = S::BX - 2, TY = S::BY - 2;
+  constexpr int NFV = S::NFV, NFH = S::NFH;
+  constexpr int NT = kStageThreads;
+  constexpr bool kBR0 = (AV == kAvBR0);
+  constexpr bool kAV = (AV != kAvNone);
+  constexpr bool U0S = (S::bRaw != S::bU0);
+
+  double* sU = tb.U;
+  double* sU0 = tb.U0;
+  const int* sEl = tb.el;
+  int* sFlag = tb.flag;
+  const double* sEps = tb.raw;
+  const double* sJx = tb.raw + NSLOT;
+  const double* sJy = tb.raw + 2 * NSLOT;
+  const double* sDx = tb.raw + 3 * NSLOT;
+  const double* sDy = tb.raw + 4 * NSLOT;
+  double* sF = smem + S::oF;
+  double* sG = smem + S::oG;
+  double* sFV = smem + S::oFV;
+  double* sFH = smem + S::oFH;
+  double* sRJ = smem + S::oDer;     // 1/(Jx Jy)
+  double* sEvx = sRJ + NSLOT;       // eps/Jx^2
+  double* sEvy = sEvx + NSLOT;      // eps/Jy^2
+  double* sRjx = sEvy + NSLOT;      // 1/Jx
+  double* sRjy = sRjx + NSLOT;      // 1/Jy
+  double* sEpsJx = sRjy + NSLOT;    // eps/Jx
+  double* sEpsJy = sEpsJx + NSLOT;  // eps/Jy
+  double* sRed = smem + S::oRed;
+
+  const int tid = threadIdx.x;
+  const int nx = M.nx;
+  const size_t cs = (size_t)M.nel * NP2;  // component stride
+  const bool prime = ctl.prime;
+  const double dt = ctl.dt, tstage = ctl.tstage;
+
+  cp_async_wait<WAIT>();
+  __syncthreads();
+  // per-element factors, once per slot instead of once per line or point
   for (int s = tid; s < NSLOT; s += NT) {
     const int el = sEl[s];
     if (el < 0) continue;
-    const int gx = el % nx, gy = el / nx;
-    sJx[s] = M.Jx[gx];
-    sJy[s] = M.Jy[gy];
-    sDx[s] = M.dx[gx];
-    sDy[s] = M.dy[gy];
-    sEps[s] = (kAV && !prime) ? B.eps_in[el] : 0.0;
+    const double jx = sJx[s], jy = sJy[s];
+    const double eps = (kAV && !prime) ? sEps[s] : 0.0;
+    sRJ[s] = 1.0 / (jx * jy);
+    if (kAV) {
+      sEvx[s] = eps / (jx * jx);
+      sEvy[s] = eps / (jy * jy);
+    }
+    if (kBR0) {
+      sRjx[s] = 1.0 / jx;
+      sRjy[s] = 1.0 / jy;
+      sEpsJx[s] = eps / jx;
+      sEpsJy[s] = eps / jy;
+    }
     if (M.solid && M.solid[el]) sFlag[s] |= kSlotSolid;
   }
-  cp_async_wait<1>();
   __syncthreads();
 
   if (!prime) {
@@ -366,8 +447,7 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
         if (kBR0) {
-          const double JA = vert ? sJx[sA] : sJy[sA], JB = vert ? sJx[sB] : sJy[sB];
-          const double sa = sEps[sA] / JA, sb = sEps[sB] / JB;
+          const double sa = vert ? sEpsJx[sA] : sEpsJy[sA], sb = vert ? sEpsJx[sB] : sEpsJy[sB];
           const double tau =
               br0_tau(sEps[sA], sEps[sB], vert ? sDx[sA] : sDy[sA], vert ? sDx[sB] : sDy[sB], P.p);
 #pragma unroll
@@ -415,8 +495,7 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
         if (kBR0) {
-          const double Jd = vert ? sJx[s] : sJy[s];
-          const double sc = sEps[s] / Jd;
+          const double sc = vert ? sEpsJx[s] : sEpsJy[s];
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) gh[c] = sc * (haveB ? gB[c] : gA[c]);
         }
@@ -459,10 +538,9 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
       const double fhE = fw[FS] - fc;
       const double ghW = kBR0 ? fw[4] : 0.0;
       const double ghE = kBR0 ? fw[FS + 4] : 0.0;
-      const double jx = sJx[s];
-      const double rJa = M.curved ? 0.0 : 1.0 / (jx * sJy[s]);
-      const double ev = kAV ? sEps[s] / (jx * jx) : 0.0;
-      const double rjx = kBR0 ? 1.0 / jx : 0.0;
+      const double rJa = M.curved ? 0.0 : sRJ[s];
+      const double ev = kAV ? sEvx[s] : 0.0;
+      const double rjx = kBR0 ? sRjx[s] : 0.0;
       const size_t mrow = (size_t)sEl[s] * NP2 + NP * j;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
@@ -515,10 +593,9 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
       const double fhN = fs[TX * FS] - gc;
       const double ghS = kBR0 ? fs[4] : 0.0;
       const double ghN = kBR0 ? fs[TX * FS + 4] : 0.0;
-      const double jy = sJy[s];
-      const double rJa = M.curved ? 0.0 : 1.0 / (sJx[s] * jy);
-      const double ev = kAV ? sEps[s] / (jy * jy) : 0.0;
-      const double rjy = kBR0 ? 1.0 / jy : 0.0;
+      const double rJa = M.curved ? 0.0 : sRJ[s];
+      const double ev = kAV ? sEvy[s] : 0.0;
+      const double rjy = kBR0 ? sRjy[s] : 0.0;
       const size_t mbase = (size_t)sEl[s] * NP2 + i;
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
@@ -541,39 +618,43 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
         Go[NP * j] = r;
       }
     }
-    cp_async_wait<0>();  // u0 prefetch has landed
     __syncthreads();
 
     // --------------------------------------------------- P5 epilogue
+    // thread (e, k): solution point k of every EL-th own element, all
+    // components (coalesced stores of whole elements).  Non-finite values
+    // are caught by accumulating v * 0, which is NaN for an infinite or NaN v.
     {
-      constexpr int OROW = TX * NP2;
-      int bad_du = 0, bad_u = 0;
+      constexpr int EL = NT / NP2;
+      const int k = tid % NP2, e = tid / NP2;
+      double chk_du = 0.0, chk_u = 0.0;
       const double cdt = B.c * dt;
-      for (int idx = tid; idx < TY * NEQ * OROW; idx += NT) {
-        const int r = idx % OROW, t = idx / OROW;
-        const int c = t % NEQ, oy = t / NEQ;
-        const int ox = r / NP2, k = r % NP2;
-        const int o = oy * TX + ox;
-        const int s = (oy + 1) * BX + ox + 1;
-        if (!(sFlag[s] & kSlotOwn)) continue;
-        const int li = o * ES + c * NP2 + k;
-        const double du = sG[li];
-        const size_t gi = c * cs + (size_t)sEl[s] * NP2 + k;
-        if (B.mode == kModeResidual) {
-          B.du_out[gi] = du;
-          bad_du |= !isfinite(du);
-          continue;
+      if (e < EL) {
+        for (int o = e; o < NOWN; o += EL) {
+          const int s = (o / TX + 1) * BX + (o % TX) + 1;
+          if (!(sFlag[s] & kSlotOwn)) continue;
+          const size_t g0 = (size_t)sEl[s] * NP2 + k;
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) {
+            const int li = o * ES + c * NP2 + k;
+            const double du = sG[li];
+            const size_t gi = c * cs + g0;
+            chk_du = fma(du, 0.0, chk_du);
+            if (B.mode == kModeResidual) {
+              B.du_out[gi] = du;
+              continue;
+            }
+            const double us = sU[s * ES + c * NP2 + k];
+            const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : __ldg(&B.u0[gi]));
+            const double un = (B.a * u0 + B.b * us) + cdt * du;
+            B.uout[gi] = un;
+            sF[li] = un;
+            chk_u = fma(un, 0.0, chk_u);
+          }
         }
-        const double us = sU[s * ES + c * NP2 + k];
-        const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : __ldg(&B.u0[gi]));
-        const double un = (B.a * u0 + B.b * us) + cdt * du;
-        B.uout[gi] = un;
-        sF[li] = un;
-        bad_du |= !isfinite(du);
-        bad_u |= !isfinite(un);
       }
-      const int any_du = __syncthreads_or(bad_du);
-      const int any_u = __syncthreads_or(bad_u);
+      const int any_du = __syncthreads_or(chk_du != chk_du);
+      const int any_u = __syncthreads_or(chk_u != chk_u);
       if (tid == 0 && (any_du || any_u)) {
         if (B.sc)
           atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
@@ -581,8 +662,6 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
     }
     if (B.mode == kModeResidual) return;
   } else {
-    cp_async_wait<0>();
-    __syncthreads();
     // prime / sense: the "new" state is the loaded state
     for (int idx = tid; idx < NOWN * NEQ * NP2; idx += NT) {
       const int o = idx % NOWN, r = idx / NOWN;
@@ -631,7 +710,7 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
       }
     }
     if (B.want_lambda) {
-      // block max of the CFL wave speed (compute_dt), one atomic per CTA
+      // block max of the CFL wave speed (compute_dt), one atomic per tile
       for (int off = 16; off > 0; off >>= 1) lmax = jmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
       if ((tid & 31) == 0) sRed[tid >> 5] = lmax;
     }
@@ -689,7 +768,23 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
   }
 }
 
-// Single solve: the grid covers the mesh with tiles.
+// One tile of one stage (single buffer).  tx0, ty0: first element of the
+// tile.  Used by stage2d_kernel and by the batched kernels.
+template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S>
+__device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
+                                             const StageBufs& B, const int tx0, const int ty0) {
+  using S = Smem2D<NP, TX, TY, U0S, MINB>;
+  extern __shared__ __align__(16) double smem[];
+  StageCtl ctl;
+  if (!stage_control(B, ctl)) return;
+  const TileBuf tb = tile_buf<S>(smem);
+  tile_slots<S>(M, tb, tx0, ty0, ctl.prime);
+  __syncthreads();
+  tile_issue<NP, AV, S>(M, B, tb, ctl);
+  tile_compute<NP, FLUX, AV, S, 0>(ops, M, P, B, tb, smem, ctl);
+}
+
+// Single solve, one tile per CTA: the grid covers the mesh with tiles.
 template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
           bool U0S = true>
 __global__ void __launch_bounds__(kStageThreads, MINB)
