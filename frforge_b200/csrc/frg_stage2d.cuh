@@ -284,24 +284,29 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 
   cp_async_wait<WAIT>();
   __syncthreads();
-  // per-element factors, once per slot instead of once per line or point
-  for (int s = tid; s < NSLOT; s += NT) {
-    const int el = sEl[s];
-    if (el < 0) continue;
-    const double jx = sJx[s], jy = sJy[s];
-    const double eps = (kAV && !prime) ? sEps[s] : 0.0;
-    sRJ[s] = 1.0 / (jx * jy);
-    if (kAV) {
-      sEvx[s] = eps / (jx * jx);
-      sEvy[s] = eps / (jy * jy);
+  // per-element factors, once per slot instead of once per line or point;
+  // one factor per thread
+  {
+    constexpr int NV = kBR0 ? 7 : (kAV ? 3 : 1);
+    for (int idx = tid; idx < NV * NSLOT; idx += NT) {
+      const int v = idx / NSLOT, s = idx % NSLOT;
+      const int el = sEl[s];
+      if (el < 0) continue;
+      const double jx = sJx[s], jy = sJy[s];
+      const double eps = (kAV && !prime) ? sEps[s] : 0.0;
+      double r;
+      switch (v) {
+        case 0: r = 1.0 / (jx * jy); break;
+        case 1: r = eps / (jx * jx); break;
+        case 2: r = eps / (jy * jy); break;
+        case 3: r = 1.0 / jx; break;
+        case 4: r = 1.0 / jy; break;
+        case 5: r = eps / jx; break;
+        default: r = eps / jy; break;
+      }
+      sRJ[v * NSLOT + s] = r;
+      if (v == 0 && M.solid && M.solid[el]) sFlag[s] |= kSlotSolid;
     }
-    if (kBR0) {
-      sRjx[s] = 1.0 / jx;
-      sRjy[s] = 1.0 / jy;
-      sEpsJx[s] = eps / jx;
-      sEpsJy[s] = eps / jy;
-    }
-    if (M.solid && M.solid[el]) sFlag[s] |= kSlotSolid;
   }
   __syncthreads();
 
@@ -508,6 +513,26 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     }
     __syncthreads();
 
+    // u0 of this thread's epilogue points, from global memory when it is not
+    // staged: issued here so that P3 and P4 cover the load latency
+    constexpr int EL5 = NT / NP2, NIT5 = (NOWN + EL5 - 1) / EL5;
+    double u0r[NIT5][NEQ];
+    if (!U0S && ctl.need_u0) {
+      const int k = tid % NP2, e = tid / NP2;
+#pragma unroll
+      for (int it = 0; it < NIT5; ++it) {
+        const int o = e + it * EL5;
+        if (e < EL5 && o < NOWN) {
+          const int s = (o / TX + 1) * BX + (o % TX) + 1;
+          if (sFlag[s] & kSlotOwn) {
+            const size_t g0 = (size_t)sEl[s] * NP2 + k;
+#pragma unroll
+            for (int c = 0; c < NEQ; ++c) u0r[it][c] = __ldg(&B.u0[c * cs + g0]);
+          }
+        }
+      }
+    }
+
     // ------------------------------------------------ P3 xi-direction
     // item = o + NOWN*(j + NP*c): lanes walk over elements
     for (int idx = tid; idx < NOWN * NP * NEQ; idx += NT) {
@@ -630,7 +655,10 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       double chk_du = 0.0, chk_u = 0.0;
       const double cdt = B.c * dt;
       if (e < EL) {
-        for (int o = e; o < NOWN; o += EL) {
+#pragma unroll
+        for (int it = 0; it < NIT5; ++it) {
+          const int o = e + it * EL;
+          if (o >= NOWN) break;
           const int s = (o / TX + 1) * BX + (o % TX) + 1;
           if (!(sFlag[s] & kSlotOwn)) continue;
           const size_t g0 = (size_t)sEl[s] * NP2 + k;
@@ -645,7 +673,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
               continue;
             }
             const double us = sU[s * ES + c * NP2 + k];
-            const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : __ldg(&B.u0[gi]));
+            const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : u0r[it][c]);
             const double un = (B.a * u0 + B.b * us) + cdt * du;
             B.uout[gi] = un;
             sF[li] = un;
