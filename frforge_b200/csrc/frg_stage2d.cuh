@@ -4,7 +4,8 @@
 // one-element halo ring (no corners) of the stage input in shared memory.
 // Everything a stage needs happens on chip:
 //   P0  cp.async copies of the tile: u_s (tile + halo), the step-start state
-//       u0 of the tile and the per-slot mesh values (eps, Jx, Jy, dx, dy)
+//       u0 of the tile and the per-slot mesh values (eps, Jx, Jy, dx, dy,
+//       h_char)
 //   P1  physical fluxes -> contravariant F~, G~ at every own solution point
 //       (Residual2D.jl:342-352)
 //   P2  every face point of the tile once: u traces of both sides
@@ -75,11 +76,11 @@ struct Smem2D {
   static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
   static constexpr int FS = odd_up(NP * 8);     // face stride: NP points x (fhat[4], ghat[4])
   // one tile buffer (doubles): u_s of tile + halo, u0 of the tile, per-slot
-  // raw mesh values [5][NSLOT] = eps, Jx, Jy, dx, dy
+  // raw mesh values [6][NSLOT] = eps, Jx, Jy, dx, dy, h_char
   static constexpr int bU = 0;
   static constexpr int bU0 = bU + NSLOT * ES;
   static constexpr int bRaw = bU0 + (U0S ? NOWN * ES : 0);
-  static constexpr int bDoubles = bRaw + 5 * NSLOT;
+  static constexpr int bDoubles = bRaw + 6 * NSLOT;
   static constexpr int oF = bDoubles;               // [NOWN][ES]
   static constexpr int oG = oF + NOWN * ES;         // [NOWN][ES]
   static constexpr int oFV = oG + NOWN * ES;        // [NFV][FS]
@@ -115,7 +116,7 @@ FRG_DEV void cp_async_wait() {
 struct TileBuf {
   double* U;    // [NSLOT][ES]
   double* U0;   // [NOWN][ES]
-  double* raw;  // [5][NSLOT]
+  double* raw;  // [6][NSLOT]
   int* el;      // [NSLOT]
   int* flag;    // [NSLOT]
 };
@@ -236,6 +237,7 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
     cp_async8(&tb.raw[2 * NSLOT + s], &M.Jy[gy]);
     cp_async8(&tb.raw[3 * NSLOT + s], &M.dx[gx]);
     cp_async8(&tb.raw[4 * NSLOT + s], &M.dy[gy]);
+    if (AV != kAvNone && (tb.flag[s] & kSlotOwn)) cp_async8(&tb.raw[5 * NSLOT + s], &M.hchar[el]);
   }
   cp_async_commit();
 }
@@ -263,6 +265,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   const double* sJy = tb.raw + 2 * NSLOT;
   const double* sDx = tb.raw + 3 * NSLOT;
   const double* sDy = tb.raw + 4 * NSLOT;
+  const double* sHc = tb.raw + 5 * NSLOT;
   double* sF = smem + S::oF;
   double* sG = smem + S::oG;
   double* sFV = smem + S::oFV;
@@ -790,7 +793,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         continue;
       }
       double ev = 0.0;
-      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (M.hchar[el] / (double)P.pm) * lam;
+      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (sHc[s] / (double)P.pm) * lam;
       B.eps_out[el] = ev;
     }
   }
