@@ -78,6 +78,15 @@ class frg_result(C.Structure):
     _fields_ = [("status", C.c_int), ("n_steps", C.c_int64), ("t", C.c_double)]
 
 
+class frg_diagnostics(C.Structure):
+    _fields_ = [("mass", C.c_double * 4), ("rho_min", C.c_double), ("rho_max", C.c_double),
+                ("p_min", C.c_double), ("nonfinite", C.c_int64), ("positivity_ok", C.c_int),
+                ("pad", C.c_int), ("l2_error", C.c_double), ("t", C.c_double)]
+
+
+EXACT = {"none": 0, "state": 1, "vortex_2d": 2, "smooth_2d": 3, "density_wave_1d": 4}
+
+
 class frg_solve_info(C.Structure):
     _fields_ = [("ndof", C.c_size_t), ("nel", C.c_int), ("np", C.c_int), ("neq", C.c_int),
                 ("device_bytes", C.c_size_t), ("residual_evals", C.c_int64), ("steps", C.c_int64)]
@@ -121,6 +130,8 @@ SIGNATURES = {
                                   C.c_int64]),
     "frg_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_result), C.POINTER(C.c_int)]),
     "frg_solve_bytes": (C.c_int, [C.POINTER(frg_solve_desc), C.POINTER(C.c_size_t)]),
+    "frg_diagnostics_compute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int,
+                                          C.POINTER(frg_diagnostics)]),
     "frg_server_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_int64, C.POINTER(C.c_void_p)]),
     "frg_server_destroy": (C.c_int, [C.c_void_p]),
     "frg_server_submit": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), _dp, C.c_double, C.c_double,
@@ -130,6 +141,7 @@ SIGNATURES = {
     "frg_server_result": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(frg_result)]),
     "frg_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int,
                                             C.POINTER(C.c_int)]),
+    "frg_server_diagnostics": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_diagnostics)]),
 }
 
 _lib = None

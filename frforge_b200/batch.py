@@ -17,7 +17,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _lib as L
-from .gpu import Context, default_context, make_desc
+from .gpu import Context, default_context, diagnostics_of, make_desc
 from .methods import AbstractCapturingMethod
 
 
@@ -108,6 +108,12 @@ class Batch:
         self._chk(L.load().frg_download_state(self._solve(slot), C.cast(host_ptr, L._dp), self._ndof[slot],
                                               C.byref(t)), "download")
         return t.value
+
+    def diagnostics(self, slot: int, exact: str = "none", t_exact: float = 0.0, c: int = 0) -> dict:
+        """Device-side scoring reductions of an instance's state (see
+        GpuSolve.diagnostics)."""
+        neq = 4 if len(self._shape[slot]) == 4 else 3
+        return diagnostics_of(self._solve(slot), self.ctx, exact, t_exact, c, 0, neq)
 
     def start(self, slot: int, t_final: float, cfl: float = 0.2, dt: Optional[float] = None,
               max_steps: int = 10**7) -> None:

@@ -38,6 +38,8 @@ struct Request {
 struct Outcome {
   int done = 0;
   frg_result r{};
+  int have_diag = 0;
+  frg_diagnostics d{};
 };
 
 }  // namespace
@@ -151,7 +153,7 @@ int frg_server_destroy(frg_server* s) {
 
 int frg_server_submit(frg_server* s, const frg_solve_desc* desc, const double* u0, double t0, double t_final,
                       double cfl, double fixed_dt, int64_t max_steps, double* u_out, int64_t* request_id) {
-  if (!s || !desc || !u0 || !u_out || !request_id) return FRG_ERR_INVALID_ARG;
+  if (!s || !desc || !u0 || !request_id) return FRG_ERR_INVALID_ARG;
   if (max_steps < 1 || (!(fixed_dt > 0.0) && !(cfl > 0.0)))
     return set_err(s->ctx, FRG_ERR_INVALID_ARG, "submit: max_steps >= 1 and cfl > 0 or dt > 0");
   Request q{};
@@ -211,9 +213,19 @@ int frg_server_pump(frg_server* s, int* n_done, int* n_queued, int* n_active) {
     if (r.status == FRG_RUNNING) continue;
     frg_solve* sv = nullptr;
     frg_batch_get_solve(s->batch, i, &sv);
-    double t = 0.0;
-    rc = frg_download_state(sv, a.u_out, a.ndof, &t);
+    // diagnostics on the device; the state itself only if the caller wants it
+    frg_diagnostics dg;
+    rc = frg_diagnostics_compute(sv, FRG_EXACT_NONE, nullptr, 0.0, 0, &dg);
+    if (!rc && a.u_out) {
+      double t = 0.0;
+      rc = frg_download_state(sv, a.u_out, a.ndof, &t);
+    }
     finish(s, a.id, rc ? rc : r.status, r.n_steps, r.t);
+    if (!rc) {
+      Outcome& o = s->outcome[a.id];
+      o.have_diag = 1;
+      o.d = dg;
+    }
     frg_batch_remove(s->batch, i);
     a.id = 0;
   }
@@ -233,6 +245,15 @@ int frg_server_result(frg_server* s, int64_t id, int* done, frg_result* r) {
   if (it == s->outcome.end()) return FRG_ERR_INVALID_ARG;
   *done = it->second.done;
   if (r) *r = it->second.r;
+  return FRG_OK;
+}
+
+int frg_server_diagnostics(frg_server* s, int64_t id, frg_diagnostics* out) {
+  if (!s || !out) return FRG_ERR_INVALID_ARG;
+  auto it = s->outcome.find(id);
+  if (it == s->outcome.end()) return FRG_ERR_INVALID_ARG;
+  if (!it->second.have_diag) return set_err(s->ctx, FRG_ERR_STATE, "request has no diagnostics (not delivered)");
+  *out = it->second.d;
   return FRG_OK;
 }
 

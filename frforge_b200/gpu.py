@@ -148,6 +148,15 @@ def make_desc(state, eq, method: Optional[AbstractCapturingMethod] = None, time:
     return d, keep
 
 
+def diagnostics_of(handle, ctx, exact: str, t_exact: float, c: int, ref_ptr: int, neq: int) -> dict:
+    d = L.frg_diagnostics()
+    L.check(L.load().frg_diagnostics_compute(handle, L.EXACT[exact], C.c_void_p(ref_ptr or None), float(t_exact),
+                                             int(c), C.byref(d)), ctx.handle, "frg_diagnostics_compute")
+    return {"mass": [d.mass[k] for k in range(neq)], "rho_min": d.rho_min, "rho_max": d.rho_max,
+            "p_min": d.p_min, "nonfinite": int(d.nonfinite), "positivity_ok": bool(d.positivity_ok),
+            "l2_error": d.l2_error, "t": d.t}
+
+
 class GpuSolve:
     """A device-resident solve (frg_solve): descriptor, state buffers, graphs."""
 
@@ -233,6 +242,14 @@ class GpuSolve:
                                        -1.0 if dt is None else float(dt), int(max_steps), C.byref(r)),
                   "frg_advance")
         return {"status": L.STATUS_SYMBOL[r.status], "n_steps": int(r.n_steps), "t": r.t}
+
+    def diagnostics(self, exact: str = "none", t_exact: float = 0.0, c: int = 0, ref_ptr: int = 0) -> dict:
+        """Device-side scoring reductions of the current state (mass per
+        component, density extrema, minimum pressure, non-finite count,
+        positivity, and the L2 error of component c against an exact
+        solution: "vortex_2d", "smooth_2d", "density_wave_1d", or "state"
+        with a device pointer ref_ptr)."""
+        return diagnostics_of(self.handle, self.ctx, exact, t_exact, c, ref_ptr, self.info()["neq"])
 
     def variant(self):
         """(current tile variant, number of variants) of the stage kernel."""

@@ -48,16 +48,18 @@ class Server:
 
     def submit(self, state, eq, method: Optional[AbstractCapturingMethod] = None, t_final: float = 1.0,
                cfl: float = 0.2, dt: Optional[float] = None, max_steps: int = 10**7,
-               time: Optional[str] = None) -> int:
+               time: Optional[str] = None, want_state: bool = True) -> int:
         """Queue ``integrate_(state, eq, method, t_final; cfl, dt, max_steps)``;
-        returns the request id."""
+        returns the request id.  want_state=False: only the device-side
+        diagnostics of the final state are returned, not the state."""
         d, keep = make_desc(state, eq, method, time)
         u0 = np.ascontiguousarray(np.asarray(state.u, dtype=np.float64).ravel(order="F"))
-        out = np.empty_like(u0)
+        out = np.empty_like(u0) if want_state else None
         rid = C.c_int64()
         self._chk(L.load().frg_server_submit(self.handle, C.byref(d), L.dptr(u0), float(state.t), float(t_final),
                                              float(cfl), -1.0 if dt is None else float(dt), int(max_steps),
-                                             L.dptr(out), C.byref(rid)), "frg_server_submit")
+                                             L.dptr(out) if want_state else None, C.byref(rid)),
+                  "frg_server_submit")
         self._req[rid.value] = (d, keep, u0, out, state.u.shape)
         return rid.value
 
@@ -93,8 +95,15 @@ class Server:
         if release:
             del self._req[rid]
         st = r.status
-        return {"status": L.STATUS_SYMBOL.get(st, st), "n_steps": int(r.n_steps), "t": r.t,
-                "u": out.reshape(shape, order="F")}
+        res = {"status": L.STATUS_SYMBOL.get(st, st), "n_steps": int(r.n_steps), "t": r.t,
+               "u": out.reshape(shape, order="F") if out is not None else None, "diagnostics": None}
+        dg = L.frg_diagnostics()
+        if L.load().frg_server_diagnostics(self.handle, int(rid), C.byref(dg)) == L.FRG_OK:
+            neq = 4 if len(shape) == 4 else 3
+            res["diagnostics"] = {"mass": [dg.mass[k] for k in range(neq)], "rho_min": dg.rho_min,
+                                  "rho_max": dg.rho_max, "p_min": dg.p_min, "nonfinite": int(dg.nonfinite),
+                                  "positivity_ok": bool(dg.positivity_ok), "t": dg.t}
+        return res
 
     def drain(self, max_pumps: int = 10**9) -> None:
         """Pump until nothing is queued or running."""

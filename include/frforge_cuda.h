@@ -292,7 +292,8 @@ int frg_server_create(frg_ctx* ctx, int slots, size_t hbm_budget, int64_t steps_
                       frg_server** out);
 int frg_server_destroy(frg_server* s);
 /* Queue one solve.  desc and every array it points to, u0 (ndof doubles,
-   host) and u_out (ndof doubles, host, written on completion) must stay
+   host) and u_out (ndof doubles, host, written on completion; NULL: the
+   final state is not downloaded, only its diagnostics are kept) must stay
    valid until the request completes.  FRG_ERR_OOM if the request alone
    exceeds the budget. */
 int frg_server_submit(frg_server* s, const frg_solve_desc* desc, const double* u0, double t0,
@@ -307,6 +308,47 @@ int frg_server_pump(frg_server* s, int* n_done, int* n_queued, int* n_active);
 int frg_server_result(frg_server* s, int64_t request_id, int* done, frg_result* r);
 /* Up to cap request ids completed since the last call, in completion order. */
 int frg_server_take_completed(frg_server* s, int64_t* ids, int cap, int* n);
+
+/* ------------------------------------------------------------ diagnostics
+   The scoring-harness reductions of the reference on the device state, so a
+   caller gets them without downloading the state:
+     mass[c]        discrete_mass(state, c+1)  (SolutionState.jl:80-90,
+                    SolutionState2D.jl:85-97)
+     rho_min/max    minimum / maximum of the density (Cases2D_Riemann.jl:111-116)
+     p_min          minimum pressure(eq, U)
+     nonfinite      number of non-finite entries (has_nonfinite, Residual.jl:219)
+     positivity_ok  positivity_ok(eq, state) (Euler.jl:62-77, Euler2D.jl:153-163)
+     l2_error       l2_error(state, uexact, c+1) (SolutionState.jl:93-107,
+                    SolutionState2D.jl:98-111) against an exact solution
+   Sums are reduced in a fixed order (deterministic), not in the reference's
+   sequential order, so they agree with it to rounding. */
+enum {
+  FRG_EXACT_NONE = 0,
+  FRG_EXACT_STATE = 1,           /* a reference state in device memory, the solve's layout */
+  FRG_EXACT_VORTEX_2D = 2,       /* isentropic_vortex_primitives, Cases2D_Riemann.jl:163-186 */
+  FRG_EXACT_SMOOTH_2D = 3,       /* the smooth order-test wave, Cases2D_Smooth.jl:124-135 */
+  FRG_EXACT_DENSITY_WAVE_1D = 4  /* euler_density_wave_conserved, Cases.jl:404-414 */
+};
+typedef struct frg_diagnostics {
+  double mass[4]; /* per component; entries beyond neq are 0 */
+  double rho_min, rho_max, p_min;
+  int64_t nonfinite;
+  int positivity_ok;
+  int pad;
+  double l2_error; /* 0 when exact == FRG_EXACT_NONE */
+  double t;        /* time of the state */
+} frg_diagnostics;
+/* exact: FRG_EXACT_*; ref_dev: device pointer for FRG_EXACT_STATE (else
+   ignored); t_exact: time of the exact solution; c: 0-based component of
+   l2_error.  2D exact solutions need point coordinates: affine or analytic
+   wavy meshes, not caller metrics. */
+int frg_diagnostics_compute(frg_solve* s, int exact, const double* ref_dev, double t_exact, int c,
+                            frg_diagnostics* out);
+
+/* Device-side diagnostics of a delivered server request's final state (see
+   frg_diagnostics_compute; no exact solution).  FRG_ERR_STATE before the
+   request completed successfully. */
+int frg_server_diagnostics(frg_server* s, int64_t request_id, frg_diagnostics* out);
 
 #ifdef __cplusplus
 }

@@ -153,3 +153,27 @@ def test_multirate_batch_matches_lockstep():
         u, _ = b.download(i)
         assert np.array_equal(u, u_solo)
     b.close()
+
+
+def test_diagnostics_without_state_download():
+    # want_state=False: the final state stays on the device; the delivered
+    # diagnostics equal those of the same request run alone in a batch
+    trace = small_trace(count=5, seed=61)
+    srv = Server(slots=3, steps_per_pump=8)
+    ids = [srv.submit(*req.build(F), t_final=req.t_final, cfl=req.cfl, want_state=False) for req in trace]
+    srv.drain()
+    for rid, req in zip(ids, trace):
+        res = srv.result(rid)
+        assert res["u"] is None and res["status"] == "ok"
+        st, eq, m = req.build(F)
+        b = Batch(capacity=1)
+        i = b.add(st, eq, m)
+        b.start(i, req.t_final, cfl=req.cfl)
+        b.run()
+        ref = b.diagnostics(i)
+        b.close()
+        got = res["diagnostics"]
+        assert got["mass"] == ref["mass"] and got["rho_min"] == ref["rho_min"]
+        assert got["rho_max"] == ref["rho_max"] and got["p_min"] == ref["p_min"]
+        assert got["positivity_ok"] and got["nonfinite"] == 0 and got["t"] == ref["t"]
+    srv.close()
