@@ -171,6 +171,25 @@ def traffic_per_launch():
     return d.get("dram_bytes_per_launch_full_c3")
 
 
+def max_over_ranks(ms: float, world: int, device: str) -> float:
+    """The slowest rank's time (every rank gets it); device: where the
+    process group's collectives run ("cuda" for NCCL, "cpu" for gloo)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, steps: int, ndof: int, ms_max: float) -> float:
+    """Whole-job DOF-stage/s of `world` replicas that each ran `steps`
+    SSP-RK3 steps (3 stages) of `ndof` DOF in at most ms_max."""
+    return world * steps * 3 * ndof / (ms_max * 1e-3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -220,12 +239,8 @@ def run_ours(args):
     barrier()
     if r["status"] != "max_steps" or r["n_steps"] != args.steps:
         raise RuntimeError(f"timed run ended early: {r}")
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * 3 * ndof / (ms_max * 1e-3)
+    ms_max = max_over_ranks(ev0.elapsed_time(ev1), world, "cuda")
+    value = replica_rate(world, args.steps, ndof, ms_max)
 
     # ---- stage-kernel roofline: CUDA events around every stage launch
     nst = max(3, min(args.steps, 30))
@@ -247,11 +262,7 @@ def run_ours(args):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * 3 * ndof / (float(t.item()) * 1e-3)
+    e2e_value = replica_rate(world, args.steps, ndof, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
     if not np.all(np.isfinite(u_out.numpy())) or r2["status"] != "max_steps":
         raise RuntimeError("e2e run produced a non-finite state")
 
