@@ -14,7 +14,8 @@
 //       and the averaged viscous flux g^ (PerssonAV2D.jl:228-350)
 //   P3  xi-direction divergence + g_DG lift (Residual2D.jl:354-374) and the
 //       BR0 / D(Du) x-terms (PerssonAV2D.jl:135-194, :352-375)
-//   P4  eta-direction terms (Residual2D.jl:376-396, PerssonAV2D.jl:376-395)
+//   P4  eta-direction terms (Residual2D.jl:376-396, PerssonAV2D.jl:376-395),
+//       independent of P3; the epilogue adds the two directions
 //   P5  SSP-RK stage combination (SSP_RK3.jl:135-164) written straight to
 //       HBM -- du never leaves the chip -- plus non-finite flags
 //   P6  sensor of the NEW state (sense!, PerssonAV2D.jl:20-59), element
@@ -591,9 +592,10 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         Fo[i] = r;
       }
     }
-    __syncthreads();
 
     // ----------------------------------------------- P4 eta-direction
+    // independent of P3 (it writes only sG): the two share one barrier
+    // interval and the epilogue adds the two directions
     for (int idx = tid; idx < NOWN * NP * NEQ; idx += NT) {
       const int o = idx % NOWN, t = idx / NOWN;
       const int i = t % NP, c = t / NP;
@@ -601,7 +603,6 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const int s = (oy + 1) * BX + ox + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
       double* Go = sG + o * ES + c * NP2 + i;
-      const double* Fo = sF + o * ES + c * NP2 + i;
       if (sFlag[s] & kSlotSolid) {
 #pragma unroll
         for (int j = 0; j < NP; ++j) Go[NP * j] = 0.0;
@@ -631,7 +632,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Gl[k];
         const double rJ = M.curved ? M.m_rJ[mbase + NP * j] : rJa;
-        double r = Fo[NP * j] - acc * rJ;
+        double r = -acc * rJ;
         if (kBR0) {
           double av = 0.0;
 #pragma unroll
@@ -668,7 +669,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) {
             const int li = o * ES + c * NP2 + k;
-            const double du = sG[li];
+            const double du = sF[li] + sG[li];
             const size_t gi = c * cs + g0;
             chk_du = fma(du, 0.0, chk_du);
             if (B.mode == kModeResidual) {
