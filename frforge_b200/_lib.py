@@ -84,6 +84,27 @@ class frg_diagnostics(C.Structure):
                 ("pad", C.c_int), ("l2_error", C.c_double), ("t", C.c_double)]
 
 
+class frg_ic(C.Structure):
+    _fields_ = [("kind", C.c_int), ("pad", C.c_int), ("x0", C.c_double), ("y0", C.c_double),
+                ("amp", C.c_double), ("phase", C.c_double), ("t", C.c_double), ("prim", (C.c_double * 4) * 4)]
+
+
+IC_KIND = {"uniform": 0, "two_state": 1, "four_quadrant": 2, "density_wave": 3, "vortex": 4, "smooth_2d": 5,
+           "shu_osher": 6}
+
+
+def make_ic(kind: str, prim=(), x0: float = 0.5, y0: float = 0.5, amp: float = 0.0, phase: float = 0.0,
+            t: float = 0.0) -> frg_ic:
+    """frg_ic of a case initial condition; prim: up to four primitive states."""
+    ic = frg_ic()
+    ic.kind = IC_KIND[kind]
+    ic.x0, ic.y0, ic.amp, ic.phase, ic.t = float(x0), float(y0), float(amp), float(phase), float(t)
+    for r, row in enumerate(prim):
+        for c, v in enumerate(row):
+            ic.prim[r][c] = float(v)
+    return ic
+
+
 EXACT = {"none": 0, "state": 1, "vortex_2d": 2, "smooth_2d": 3, "density_wave_1d": 4}
 
 
@@ -130,6 +151,9 @@ SIGNATURES = {
                                   C.c_int64]),
     "frg_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_result), C.POINTER(C.c_int)]),
     "frg_solve_bytes": (C.c_int, [C.POINTER(frg_solve_desc), C.POINTER(C.c_size_t)]),
+    "frg_set_initial_condition": (C.c_int, [C.c_void_p, C.POINTER(frg_ic)]),
+    "frg_server_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(frg_ic), C.c_double,
+                                       C.c_double, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]),
     "frg_diagnostics_compute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int,
                                           C.POINTER(frg_diagnostics)]),
     "frg_server_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_int64, C.POINTER(C.c_void_p)]),

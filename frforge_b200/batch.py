@@ -109,6 +109,12 @@ class Batch:
                                               C.byref(t)), "download")
         return t.value
 
+    def set_initial_condition(self, slot: int, kind: str, prim=(), x0: float = 0.5, y0: float = 0.5,
+                              amp: float = 0.0, phase: float = 0.0, t: float = 0.0) -> None:
+        """Evaluate a case IC on the device into the instance's state (time 0)."""
+        ic = L.make_ic(kind, prim, x0, y0, amp, phase, t)
+        self._chk(L.load().frg_set_initial_condition(self._solve(slot), C.byref(ic)), "frg_set_initial_condition")
+
     def diagnostics(self, slot: int, exact: str = "none", t_exact: float = 0.0, c: int = 0) -> dict:
         """Device-side scoring reductions of an instance's state (see
         GpuSolve.diagnostics)."""

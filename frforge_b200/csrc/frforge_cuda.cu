@@ -329,14 +329,6 @@ int validate(frg_ctx* c, const frg_solve_desc* d) {
 }
 
 // analytic wavy map partials, MeshMetrics2D.jl:310-318
-void wavy_partials(double X, double Y, double a, double* xX, double* xY, double* yX, double* yY) {
-  const double tp = 6.283185307179586, pi = 3.141592653589793;
-  *xX = 1.0 + a * std::sin(tp * Y) * pi * std::cos(pi * X);
-  *xY = a * tp * std::cos(tp * Y) * std::sin(pi * X);
-  *yX = a * tp * std::cos(tp * X) * std::sin(pi * Y);
-  *yY = 1.0 + a * std::sin(tp * X) * pi * std::cos(pi * Y);
-}
-
 int setup_2d(frg_solve* s, const frg_solve_desc* d) {
   const int nx = d->nx, ny = d->ny, np = s->np, nel = nx * ny;
   std::vector<double> xv(nx + 1), yv(ny + 1);
@@ -399,52 +391,40 @@ int setup_2d(frg_solve* s, const frg_solve_desc* d) {
   // curved: per-SP metric fields (element-major [e][k]) and face normals
   M.curved = 1;
   const size_t nsp = (size_t)nel * np * np, nfp = (size_t)nel * np;
+  if (d->geometry == FRG_GEOM_WAVY) {
+    // build_mesh_metrics_analytic_wavy (MeshMetrics2D.jl:327-442), evaluated
+    // on the device straight into the metric arrays
+    double *dxxi, *dxeta, *dyxi, *dyeta, *drJ, *fdev[3][4];
+    if ((rc = dev_alloc(s, &dxxi, nsp)) || (rc = dev_alloc(s, &dxeta, nsp)) || (rc = dev_alloc(s, &dyxi, nsp)) ||
+        (rc = dev_alloc(s, &dyeta, nsp)) || (rc = dev_alloc(s, &drJ, nsp)))
+      return rc;
+    for (int a = 0; a < 3; ++a)
+      for (int f = 0; f < 4; ++f)
+        if ((rc = dev_alloc(s, &fdev[a][f], nfp))) return rc;
+    const int e = launch_wavy_metrics(nel, nx, np, M.xc, M.Jx, M.yc, M.Jy, s->ops.xi, d->wavy_amp, dxxi, dxeta,
+                                      dyxi, dyeta, drJ, fdev[0], fdev[1], fdev[2], s->ctx->stream);
+    if (e) return cuda_err(s->ctx, (cudaError_t)e, "wavy metrics");
+    if ((rc = dev_upload(s, &p, hchar.data(), nel))) return rc;
+    M.hchar = p;
+    s->hmin = hchar[0];
+    for (int k = 1; k < nel; ++k) s->hmin = std::fmin(s->hmin, hchar[k]);
+    M.m_xxi = dxxi;
+    M.m_xeta = dxeta;
+    M.m_yxi = dyxi;
+    M.m_yeta = dyeta;
+    M.m_rJ = drJ;
+    for (int f = 0; f < 4; ++f) {
+      M.f_nx[f] = fdev[0][f];
+      M.f_ny[f] = fdev[1][f];
+      M.f_sJ[f] = fdev[2][f];
+    }
+    return FRG_OK;
+  }
   std::vector<double> xxi(nsp), xeta(nsp), yxi(nsp), yeta(nsp), rJ(nsp);
   std::vector<double> fn[3][4];
   for (int a = 0; a < 3; ++a)
     for (int f = 0; f < 4; ++f) fn[a][f].resize(nfp);
-  if (d->geometry == FRG_GEOM_WAVY) {
-    // build_mesh_metrics_analytic_wavy, MeshMetrics2D.jl:327-442
-    const double amp = d->wavy_amp;
-    for (int e = 0; e < nel; ++e) {
-      const int jx = e % nx, jy = e / nx;
-      for (int j = 0; j < np; ++j)
-        for (int i = 0; i < np; ++i) {
-          const double X = xc[jx] + Jx[jx] * s->ops.xi[i], Y = yc[jy] + Jy[jy] * s->ops.xi[j];
-          double a, b, c2, d2;
-          wavy_partials(X, Y, amp, &a, &b, &c2, &d2);
-          const size_t k = (size_t)e * np * np + i + np * j;
-          xxi[k] = a * Jx[jx];
-          xeta[k] = b * Jy[jy];
-          yxi[k] = c2 * Jx[jx];
-          yeta[k] = d2 * Jy[jy];
-          rJ[k] = 1.0 / (xxi[k] * yeta[k] - xeta[k] * yxi[k]);
-        }
-      for (int q = 0; q < np; ++q) {
-        const size_t k = (size_t)e * np + q;
-        const double Y = yc[jy] + Jy[jy] * s->ops.xi[q], X = xc[jx] + Jx[jx] * s->ops.xi[q];
-        double a, b, c2, d2;
-        // west / east: n ~ (-y_eta, x_eta) / (y_eta, -x_eta)
-        for (int side = 0; side < 2; ++side) {
-          wavy_partials(xc[jx] + Jx[jx] * (side ? 1.0 : -1.0), Y, amp, &a, &b, &c2, &d2);
-          const double xe = b * Jy[jy], ye = d2 * Jy[jy];
-          const double sJ = std::fmax(std::sqrt(ye * ye + xe * xe), kEps);
-          fn[0][side][k] = side ? ye / sJ : -ye / sJ;
-          fn[1][side][k] = side ? -xe / sJ : xe / sJ;
-          fn[2][side][k] = sJ;
-        }
-        // south / north: n ~ (y_xi, -x_xi) / (-y_xi, x_xi)
-        for (int side = 0; side < 2; ++side) {
-          wavy_partials(X, yc[jy] + Jy[jy] * (side ? 1.0 : -1.0), amp, &a, &b, &c2, &d2);
-          const double xx = a * Jx[jx], yx = c2 * Jx[jx];
-          const double sJ = std::fmax(std::sqrt(yx * yx + xx * xx), kEps);
-          fn[0][2 + side][k] = side ? -yx / sJ : yx / sJ;
-          fn[1][2 + side][k] = side ? xx / sJ : -xx / sJ;
-          fn[2][2 + side][k] = sJ;
-        }
-      }
-    }
-  } else {
+  {
     const frg_metrics2d* m = d->metrics;
     const double* srcf[3][4] = {{m->nx_W, m->nx_E, m->nx_S, m->nx_N},
                                 {m->ny_W, m->ny_E, m->ny_S, m->ny_N},

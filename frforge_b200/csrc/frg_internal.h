@@ -164,6 +164,14 @@ struct BatchStatus {
   double t;
 };
 
+// ---- device set-up (frg_setup.cu) ----
+// analytic wavy metrics (MeshMetrics2D.jl:327-442) into device arrays;
+// returns 0 or a CUDA error code
+int launch_wavy_metrics(int nel, int nx, int np, const double* xc, const double* Jx, const double* yc,
+                        const double* Jy, const double* xi, double amp, double* xxi, double* xeta, double* yxi,
+                        double* yeta, double* rJ, double* const fnx[4], double* const fny[4],
+                        double* const fsJ[4], void* stream);
+
 // ---- host helpers (frg_host.cpp) ----
 int build_host_ops(int p, int points, HostOps* out);
 int host_ops_from_caller(const frg_operators* in, HostOps* out);

@@ -27,7 +27,8 @@ namespace {
 struct Request {
   int64_t id;
   frg_solve_desc desc;
-  const double* u0;
+  const double* u0;  // NULL: the state comes from ic on the device
+  frg_ic ic;
   double t0, t_final, cfl, fixed_dt;
   int64_t max_steps;
   double* u_out;
@@ -104,7 +105,7 @@ int admit(frg_server* s) {
     }
     frg_solve* sv = nullptr;
     frg_batch_get_solve(s->batch, slot, &sv);
-    rc = frg_upload_state(sv, q.u0, q.ndof, q.t0);
+    rc = q.u0 ? frg_upload_state(sv, q.u0, q.ndof, q.t0) : frg_set_initial_condition(sv, &q.ic);
     if (!rc) rc = frg_batch_start(s->batch, slot, q.t_final, q.cfl, q.fixed_dt, q.max_steps);
     if (rc) {
       frg_batch_remove(s->batch, slot);
@@ -173,6 +174,20 @@ int frg_server_submit(frg_server* s, const frg_solve_desc* desc, const double* u
   s->outcome[q.id] = Outcome{};
   s->queue.push_back(q);
   *request_id = q.id;
+  return FRG_OK;
+}
+
+// As frg_server_submit, with the initial state evaluated on the device at
+// admission (frg_set_initial_condition) instead of uploaded.
+int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic* ic, double t_final, double cfl,
+                         double fixed_dt, int64_t max_steps, double* u_out, int64_t* request_id) {
+  if (!s || !desc || !ic || !request_id) return FRG_ERR_INVALID_ARG;
+  static const double dummy = 0.0;
+  int rc = frg_server_submit(s, desc, &dummy, 0.0, t_final, cfl, fixed_dt, max_steps, u_out, request_id);
+  if (rc) return rc;
+  Request& q = s->queue.back();
+  q.u0 = nullptr;
+  q.ic = *ic;
   return FRG_OK;
 }
 

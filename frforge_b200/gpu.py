@@ -243,6 +243,13 @@ class GpuSolve:
                   "frg_advance")
         return {"status": L.STATUS_SYMBOL[r.status], "n_steps": int(r.n_steps), "t": r.t}
 
+    def set_initial_condition(self, kind: str, prim=(), x0: float = 0.5, y0: float = 0.5, amp: float = 0.0,
+                              phase: float = 0.0, t: float = 0.0) -> None:
+        """set_initial_condition! for a case IC, evaluated on the device
+        (see frg_ic in include/frforge_cuda.h); the state time becomes 0."""
+        ic = L.make_ic(kind, prim, x0, y0, amp, phase, t)
+        self._chk(L.load().frg_set_initial_condition(self.handle, C.byref(ic)), "frg_set_initial_condition")
+
     def diagnostics(self, exact: str = "none", t_exact: float = 0.0, c: int = 0, ref_ptr: int = 0) -> dict:
         """Device-side scoring reductions of the current state (mass per
         component, density extrema, minimum pressure, non-finite count,

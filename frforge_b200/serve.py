@@ -63,6 +63,23 @@ class Server:
         self._req[rid.value] = (d, keep, u0, out, state.u.shape)
         return rid.value
 
+    def submit_ic(self, state, eq, ic: dict, method: Optional[AbstractCapturingMethod] = None,
+                  t_final: float = 1.0, cfl: float = 0.2, dt: Optional[float] = None, max_steps: int = 10**7,
+                  time: Optional[str] = None, want_state: bool = True) -> int:
+        """As submit, with the initial state evaluated on the device at
+        admission from the case IC ``ic`` (keyword arguments of
+        frforge_b200._lib.make_ic); ``state`` gives the mesh and scheme only."""
+        d, keep = make_desc(state, eq, method, time)
+        c_ic = L.make_ic(**ic)
+        out = np.empty(int(np.prod(state.u.shape))) if want_state else None
+        rid = C.c_int64()
+        self._chk(L.load().frg_server_submit_ic(self.handle, C.byref(d), C.byref(c_ic), float(t_final), float(cfl),
+                                                -1.0 if dt is None else float(dt), int(max_steps),
+                                                L.dptr(out) if want_state else None, C.byref(rid)),
+                  "frg_server_submit_ic")
+        self._req[rid.value] = (d, keep, None, out, state.u.shape)
+        return rid.value
+
     def cancel(self, rid: int) -> None:
         self._chk(L.load().frg_server_cancel(self.handle, int(rid)), "frg_server_cancel")
 

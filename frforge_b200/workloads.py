@@ -110,7 +110,7 @@ class Workload2D:
             phi = uniform(g, 0.0, 2 * math.pi)
             r = 1.0 + 0.2 * np.sin(2 * math.pi * (X + Y) + phi)
             one = np.ones_like(r)
-            return np.stack([r, r, r, one / 0.4 + 0.5 * r * 2.0], axis=-1)
+            return np.stack([r, r, r, one / (1.4 - 1.0) + 0.5 * r * (1.0 * 1.0 + 1.0 * 1.0)], axis=-1)
         return four_quadrant_ic(X, Y, four_quadrant_states(self.seed, self.jump_scale))
 
 
@@ -159,6 +159,23 @@ class Request:
     def ndof(self) -> int:
         return self.n * self.n * (self.p + 1) ** 2 * 4 if self.dim == 2 else self.n * (self.p + 1) * 3
 
+    def ic(self) -> dict:
+        """The request's initial condition as a device-side case IC
+        (keyword arguments of frforge_b200._lib.make_ic): the same state
+        build() evaluates on the host."""
+        g = splitmix64(self.seed)
+        if self.periodic:
+            phi = uniform(g, 0.0, 2 * math.pi)
+            prim = [(1.0, 1.0, 1.0)] if self.dim == 1 else [(1.0, 1.0, 1.0, 1.0)]
+            return dict(kind="density_wave", prim=prim, amp=0.2, phase=phi)
+        if self.dim == 1:
+            L, R = two_state_1d(self.seed)
+            m = [(a + b) / 2.0 for a, b in zip(L, R)]
+            L = [mm + 0.25 * (a - mm) for mm, a in zip(m, L)]
+            R = [mm + 0.25 * (b - mm) for mm, b in zip(m, R)]
+            return dict(kind="two_state", prim=[L, R], x0=0.5)
+        return dict(kind="four_quadrant", prim=four_quadrant_states(self.seed, 0.25), x0=0.5, y0=0.5)
+
     def build(self, F):
         """(state, eq, method) for the frforge_b200 module F, IC filled in."""
         g = splitmix64(self.seed)
@@ -180,7 +197,7 @@ class Request:
                 r = np.where(X < 0.5, L[0], R[0])
                 u = np.where(X < 0.5, L[1], R[1])
                 p = np.where(X < 0.5, L[2], R[2])
-            st.u[...] = np.stack([r, r * u, p / 0.4 + 0.5 * r * u * u], axis=-1)
+            st.u[...] = np.stack([r, r * u, p / (1.4 - 1.0) + 0.5 * r * u * u], axis=-1)
             return st, F.Euler1D(1.4), method
         if self.wavy:
             mesh = F.make_wavy_mesh2d(self.n, self.n, amp=0.05, left_bc=bc(), right_bc=bc(), bottom_bc=bc(),

@@ -350,6 +350,45 @@ int frg_diagnostics_compute(frg_solve* s, int exact, const double* ref_dev, doub
    request completed successfully. */
 int frg_server_diagnostics(frg_server* s, int64_t request_id, frg_diagnostics* out);
 
+/* ------------------------------------------------------ initial conditions
+   set_initial_condition! (SolutionState.jl:59-73, SolutionState2D.jl:58-82)
+   for the reference's case initial conditions, evaluated on the device at
+   the solution points (physical_xy, MeshMetrics2D.jl:49-74, including the
+   analytic wavy map), so a request needs no host evaluation or upload of
+   its state.  Sets the state time to 0.  prim rows are primitive states
+   (rho, u, v, p) in 2D, (rho, u, p) in 1D:
+     UNIFORM        prim[0]
+     TWO_STATE      x < x0 ? prim[0] : prim[1]  (sod_ic, Cases.jl:940-946)
+     FOUR_QUADRANT  riemann2d_ic quadrant rule at (x0, y0), prim = ne, nw, sw, se
+                    (Cases2D_Riemann.jl:33-51)
+     DENSITY_WAVE   prim[0] with rho = prim[0][0] + amp sin(2 pi (x [+ y] - t) + phase)
+                    (euler_density_wave_conserved, Cases.jl:404-414)
+     VORTEX         isentropic_vortex_primitives at time t (Cases2D_Riemann.jl:163-186)
+     SMOOTH_2D      the smooth order-test wave at time t (Cases2D_Smooth.jl:124-135)
+     SHU_OSHER      shu_osher_ic (Cases.jl:930-938), 1D */
+enum {
+  FRG_IC_UNIFORM = 0,
+  FRG_IC_TWO_STATE = 1,
+  FRG_IC_FOUR_QUADRANT = 2,
+  FRG_IC_DENSITY_WAVE = 3,
+  FRG_IC_VORTEX = 4,
+  FRG_IC_SMOOTH_2D = 5,
+  FRG_IC_SHU_OSHER = 6
+};
+typedef struct frg_ic {
+  int kind; /* FRG_IC_* */
+  int pad;
+  double x0, y0, amp, phase, t;
+  double prim[4][4];
+} frg_ic;
+int frg_set_initial_condition(frg_solve* s, const frg_ic* ic);
+/* frg_server_submit with the initial state evaluated on the device at
+   admission (frg_set_initial_condition) instead of uploaded; the state time
+   starts at 0. */
+int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic* ic, double t_final,
+                         double cfl, double fixed_dt, int64_t max_steps, double* u_out,
+                         int64_t* request_id);
+
 #ifdef __cplusplus
 }
 #endif
