@@ -426,9 +426,10 @@ def run_served(args):
     """A seeded Poisson request trace (frforge_b200.workloads.served_trace:
     1D and 2D solves, P 1..5, wavy 2D meshes, t_final U[0.05, 0.25]) served by
     frg_server_* against the same requests served one at a time (FIFO,
-    frg_solve_create + frg_advance + download per request).  Latency is
-    arrival -> final state on the host, on the host clock; both arms include
-    the device set-up of every solve (initial states are built beforehand)."""
+    frg_solve_create + device IC + frg_advance + download per request).
+    Latency is arrival -> final state on the host, on the host clock; both
+    arms include the device set-up of every solve and evaluate its initial
+    condition on the device."""
     import torch
 
     import frforge_b200 as F
@@ -439,7 +440,9 @@ def run_served(args):
     torch.cuda.set_device(local)
     ctx = F.Context(local)
     trace = served_trace(count=args.served_requests)
-    built = [req.build(F) for req in trace]
+    # mesh and scheme only: both arms evaluate each request's IC on the device
+    built = [req.build(F, fill=False) for req in trace]
+    ics = [req.ic() for req in trace]
     arrivals = np.array([r.arrival for r in trace])
 
     def served_arm():
@@ -450,7 +453,7 @@ def run_served(args):
             now = time.perf_counter() - t0
             while nxt < len(trace) and arrivals[nxt] <= now:
                 st, eq, m = built[nxt]
-                ids.append(srv.submit(st, eq, m, t_final=trace[nxt].t_final, cfl=trace[nxt].cfl))
+                ids.append(srv.submit_ic(st, eq, ics[nxt], m, t_final=trace[nxt].t_final, cfl=trace[nxt].cfl))
                 nxt += 1
             _, q, a = srv.pump()
             now = time.perf_counter() - t0
@@ -472,7 +475,7 @@ def run_served(args):
                 time.sleep(arrivals[k] - now)
             st, eq, m = built[k]
             s = F.GpuSolve(st, eq, m, ctx=ctx)
-            s.upload(st.u, 0.0)
+            s.set_initial_condition(**ics[k])
             r = s.advance(req.t_final, cfl=req.cfl)
             u, _ = s.download()
             s.close()
@@ -522,9 +525,9 @@ def run_served(args):
         "max_rel_linf_vs_sequential": worst,
         "max_rel_l1_vs_sequential": worst_l1,
         "statuses": {st: sum(1 for r in res_s if r["status"] == st) for st in sorted({r["status"] for r in res_s})},
-        "e2e": {"value": len(trace) / span_s, "unit": "solves/s",
-                "h2d_bytes_per_step": 8 * sum(req.ndof for req in trace) / max(steps, 1),
-                "d2h_bytes_per_step": 8 * sum(req.ndof for req in trace) / max(steps, 1)},
+        "e2e": {"value": len(trace) / span_s, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * sum(req.ndof for req in trace) / max(steps, 1),
+                "note": "initial states evaluated on the device (frg_server_submit_ic); final states downloaded"},
         "clocks": clk.summary(),
     }
     print(json.dumps(line))

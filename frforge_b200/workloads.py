@@ -176,8 +176,10 @@ class Request:
             return dict(kind="two_state", prim=[L, R], x0=0.5)
         return dict(kind="four_quadrant", prim=four_quadrant_states(self.seed, 0.25), x0=0.5, y0=0.5)
 
-    def build(self, F):
-        """(state, eq, method) for the frforge_b200 module F, IC filled in."""
+    def build(self, F, fill: bool = True):
+        """(state, eq, method) for the frforge_b200 module F, IC filled in
+        (fill=False: mesh and scheme only, the state left zero, for a
+        device-side IC)."""
         g = splitmix64(self.seed)
         ops = F.build_operators(self.p)
         method = F.PerssonAVMethod(c_av=0.1)
@@ -185,6 +187,8 @@ class Request:
         if self.dim == 1:
             mesh = F.Mesh1D(0.0, 1.0, self.n, bc(), bc())
             st = F.allocate_state(mesh, ops, 3, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+            if not fill:
+                return st, F.Euler1D(1.4), method
             X = mesh.physical_coords(ops)
             if self.periodic:
                 phi = uniform(g, 0.0, 2 * math.pi)
@@ -205,6 +209,8 @@ class Request:
         else:
             mesh = F.Mesh2D(0.0, 1.0, 0.0, 1.0, self.n, self.n, bc(), bc(), bc(), bc())
         st = F.allocate_state(mesh, ops, 4, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+        if not fill:
+            return st, F.Euler2D(1.4), method
         X, Y = mesh.physical_coords(ops)
         w = Workload2D("c2" if self.periodic else "c3", self.n, self.p, self.flux, "persson_av", 0.1,
                        self.periodic, self.cfl, 0, seed=self.seed)
