@@ -314,6 +314,13 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   }
   __syncthreads();
 
+  // wave speeds of the new state (P5 in a stage, P6 in prime / sense), in the
+  // face-array space, which is free once P3 and P4 are done
+  constexpr int WS = odd_up(NP2);
+  double* sWS = sFV;  // [NOWN][WS]
+  const bool need_ws = kAV || B.want_lambda || B.mode == kModeSense;
+  double lmax = 0.0;
+
   if (!prime) {
     // ------------------------------------------------------- P1 fluxes
     // item = o + NOWN*k: lanes walk over elements
@@ -666,6 +673,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           const int s = (o / TX + 1) * BX + (o % TX) + 1;
           if (!(sFlag[s] & kSlotOwn)) continue;
           const size_t g0 = (size_t)sEl[s] * NP2 + k;
+          double unv[NEQ];
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) {
             const int li = o * ES + c * NP2 + k;
@@ -681,7 +689,14 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
             const double un = (B.a * u0 + B.b * us) + cdt * du;
             B.uout[gi] = un;
             sF[li] = un;
+            unv[c] = un;
             chk_u = fma(un, 0.0, chk_u);
+          }
+          // wave speed of the new state at this point (P6 uses it)
+          if (B.mode != kModeResidual && need_ws) {
+            const double w = wave_speed2(P.gamma, P.g1, unv);
+            sWS[o * WS + k] = w;
+            lmax = jmax(lmax, w);
           }
         }
       }
@@ -706,12 +721,11 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   // ------------------------------------------ P6 sensor / eps / lambda
   if (!(kAV || B.want_lambda || B.mode == kModeSense)) return;
   {
-    constexpr int WS = odd_up(NP2), PS = odd_up(2 * NP);
-    double* sWS = sG;                // [NOWN][WS] wave speeds
-    double* sX = sG + NOWN * WS;     // [NOWN][WS] V^{-1} rho
+    constexpr int PS = odd_up(2 * NP);
+    double* sX = sG;                 // [NOWN][WS] V^{-1} rho
     double* sPart = sX + NOWN * WS;  // [NOWN][PS] row energies
-    double lmax = 0.0;
-    for (int idx = tid; idx < NOWN * NP2; idx += NT) {
+    // in a stage the epilogue computed the wave speeds
+    for (int idx = tid; prime && idx < NOWN * NP2; idx += NT) {
       const int o = idx % NOWN, k = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
