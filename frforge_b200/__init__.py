@@ -18,6 +18,8 @@ from .operators import FROperators, build_operators, n_points
 from .scheme import DEFAULT_SCHEME, SchemeConfig, parse_scheme, scheme_dict
 from .state import (SolutionState, SolutionState2D, allocate_state, discrete_mass, has_nonfinite,
                     positivity_ok, set_initial_condition_, solution_extrema)
+from .vtk import (VTK_LAGRANGE_LINE, VTK_LAGRANGE_QUAD, write_vtu_high_order,
+                  write_vtu_high_order_with_capturing)
 from ._lib import FRGError, UnsupportedHookError
 
 __all__ = [n for n in dir() if not n.startswith("_")]
