@@ -105,6 +105,20 @@ def make_ic(kind: str, prim=(), x0: float = 0.5, y0: float = 0.5, amp: float = 0
     return ic
 
 
+HOOK_SLOT = {"post_step": 0}
+
+
+def device_hooks() -> dict:
+    """Registered device hook implementations: name -> (slot, id, nparams)."""
+    out = {}
+    lib = load()
+    for i in range(lib.frg_hook_count()):
+        name, slot, hid, npar = C.c_char_p(), C.c_int(), C.c_int(), C.c_int()
+        lib.frg_hook_info(i, C.byref(name), C.byref(slot), C.byref(hid), C.byref(npar))
+        out[name.value.decode()] = (slot.value, hid.value, npar.value)
+    return out
+
+
 EXACT = {"none": 0, "state": 1, "vortex_2d": 2, "smooth_2d": 3, "density_wave_1d": 4}
 
 
@@ -152,6 +166,12 @@ SIGNATURES = {
     "frg_batch_run": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_result), C.POINTER(C.c_int)]),
     "frg_solve_bytes": (C.c_int, [C.POINTER(frg_solve_desc), C.POINTER(C.c_size_t)]),
     "frg_set_initial_condition": (C.c_int, [C.c_void_p, C.POINTER(frg_ic)]),
+    "frg_hook_count": (C.c_int, []),
+    "frg_hook_info": (C.c_int, [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_int)]),
+    "frg_hook_lookup": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "frg_solve_set_hook": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int]),
+    "frg_apply_post_step": (C.c_int, [C.c_void_p]),
     "frg_server_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(frg_ic), C.c_double,
                                        C.c_double, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]),
     "frg_diagnostics_compute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int,

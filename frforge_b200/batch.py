@@ -30,6 +30,13 @@ def solve_bytes(state, eq, method: Optional[AbstractCapturingMethod] = None,
     return int(n.value)
 
 
+def _refuse_hooks(method) -> None:
+    """Batched instances run no device hooks (frg_batch_start refuses them)."""
+    if method is not None and method.gpu_spec().get("hooks"):
+        raise L.UnsupportedHookError(L.FRG_ERR_UNSUPPORTED_HOOK,
+                                     f"{type(method).__name__}: batched instances run no post-step hook")
+
+
 class Batch:
     """A set of instance slots advanced together (``frg_batch``)."""
 
@@ -73,6 +80,7 @@ class Batch:
         """Create an instance for ``state`` (its u and t are uploaded); returns
         its slot.  Raises FRGError (FRG_ERR_OOM) when the batch is full or its
         HBM budget would be exceeded."""
+        _refuse_hooks(method)
         d, _keep = make_desc(state, eq, method, time, caller_ops)
         slot = C.c_int()
         self._chk(L.load().frg_batch_add(self.handle, C.byref(d), C.byref(slot)), "frg_batch_add")

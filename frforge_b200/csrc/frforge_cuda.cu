@@ -240,7 +240,9 @@ int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
   }
   step_end_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc, rk2 ? 2 : 3);
   cudaError_t e = cudaGetLastError();
-  return cuda_err(s->ctx, e, "control kernel");
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "control kernel");
+  // post_step!(state, method, eq) of a completed step (SSP_RK3.jl:162)
+  return enqueue_post_step(s, false);
 }
 
 // Copy buffer `src` into the canonical state buffer 0 after a divergence.

@@ -485,6 +485,7 @@ int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixe
   if (!b || i < 0 || i >= b->cap || !b->slot[i]) return FRG_ERR_INVALID_ARG;
   frg_solve* s = b->slot[i];
   if (!s->have_state) return set_err(b->ctx, FRG_ERR_STATE, "no state uploaded");
+  if (s->post_step_id) return set_err(b->ctx, FRG_ERR_UNSUPPORTED_HOOK, "batched instances run no post-step hook");
   if (max_steps < 1 || (!(fixed_dt > 0.0) && !(cfl > 0.0))) return set_err(b->ctx, FRG_ERR_INVALID_ARG, "run");
   cudaSetDevice(b->ctx->device);
   int rc = make_current_canonical(s);

@@ -10,6 +10,7 @@ namespace frg {
 // Top of the ssp_rk3!/ssp_rk2! loop body (SSP_RK3.jl:185-189): loop test,
 // dt from the CFL wave speed of the current state, last-step clipping.
 __device__ __forceinline__ void step_begin_device(DevScalars* sc) {
+  sc->stepped_ok = 0;
   if (sc->status != kRunning) {
     sc->active = 0;
     return;
@@ -63,6 +64,7 @@ __device__ __forceinline__ void step_end_device(DevScalars* sc, int nstages) {
     return;
   }
   sc->t = t0 + dt;
+  sc->stepped_ok = 1;
   if (sc->n_steps >= sc->max_steps) sc->status = FRG_MAX_STEPS;
 }
 

@@ -1,0 +1,230 @@
+// Device hook registry: compiled implementations of capturing-method hooks
+// that a method selects by name, so that a method overriding a hook can run
+// on the GPU instead of being rejected with FRG_ERR_UNSUPPORTED_HOOK.  The
+// reference's hooks are Julia functions dispatched on the method type
+// (src/capturing/Interfaces.jl:43-92); a solve here carries at most one
+// implementation per hook slot, chosen with frg_solve_set_hook.
+//
+// Registered implementations:
+//   post_step "positivity_zhang_shu"  the positivity-preserving scaling of
+//       Zhang & Shu (J. Comput. Phys. 229 (2010) 8918-8934): per element,
+//       the density at every solution point is pulled toward the element
+//       mean until it is >= eps_rho, then all components are pulled toward
+//       the mean by the largest theta in [0, 1] that keeps the pressure
+//       >= eps_p at every point (the exact root of the pressure quadratic
+//       along u_mean + t (u_k - u_mean)).  Element means use the quadrature
+//       weights w_i w_j |J|, so the element integrals -- and the discrete
+//       mass -- are unchanged.  Elements whose mean is not admissible are
+//       left as they are.  params: eps_rho, eps_p (defaults 1e-13).
+//
+// Time-loop placement (ssp_rk3_step!, SSP_RK3.jl:135-164): post_step! runs
+// after every step that did not diverge, before the next compute_dt; here
+// the hook kernel runs after the step's end kernel when the step completed,
+// and a prime pass recomputes the element viscosity and the CFL wave speed
+// of the limited state.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "frg_device.cuh"
+#include "frg_runtime.h"
+
+namespace frg {
+namespace {
+
+struct HookEntry {
+  const char* name;
+  int slot;
+  int id;
+  int nparams;
+};
+const HookEntry kHooks[] = {
+    {"positivity_zhang_shu", FRG_HOOK_POST_STEP, kHookPositivity, 2},
+};
+constexpr int kNumHooks = (int)(sizeof(kHooks) / sizeof(kHooks[0]));
+
+struct Weights {
+  double w[kMaxNp];
+};
+
+// smallest root in [0, 1] of a t^2 + b t + c with c > 0 >= a + b + c
+__device__ double root01(double a, double b, double c) {
+  if (fabs(a) < 1e-300) return b != 0.0 ? fmin(fmax(-c / b, 0.0), 1.0) : 0.0;
+  const double disc = fmax(b * b - 4.0 * a * c, 0.0);
+  const double q = -0.5 * (b + copysign(sqrt(disc), b));
+  double r1 = q / a, r2 = q != 0.0 ? c / q : 2.0;
+  double t = 1.0;
+  if (r1 >= 0.0 && r1 <= 1.0) t = fmin(t, r1);
+  if (r2 >= 0.0 && r2 <= 1.0) t = fmin(t, r2);
+  return t;
+}
+
+template <int NEQ>
+__device__ void zs_element(double* u, size_t n, size_t base, int npts, const double* ww, double g1, double er,
+                           double ep) {
+  double mean[NEQ], wsum = 0.0;
+  for (int c = 0; c < NEQ; ++c) mean[c] = 0.0;
+  for (int k = 0; k < npts; ++k) {
+    wsum += ww[k];
+    for (int c = 0; c < NEQ; ++c) mean[c] += ww[k] * u[c * n + base + k];
+  }
+  for (int c = 0; c < NEQ; ++c) mean[c] /= wsum;
+  const double mm2 = NEQ == 4 ? mean[1] * mean[1] + mean[2] * mean[2] : mean[1] * mean[1];
+  const double pbar = g1 * (mean[NEQ - 1] - 0.5 * mm2 / mean[0]);
+  if (!(mean[0] > er) || !(pbar > ep)) return;  // mean not admissible
+  // density
+  double rmin = mean[0];
+  for (int k = 0; k < npts; ++k) rmin = fmin(rmin, u[base + k]);
+  if (rmin < er) {
+    const double th = (mean[0] - er) / (mean[0] - rmin);
+    for (int k = 0; k < npts; ++k) u[base + k] = mean[0] + th * (u[base + k] - mean[0]);
+  }
+  // pressure
+  double theta = 1.0;
+  for (int k = 0; k < npts; ++k) {
+    double U[NEQ];
+    for (int c = 0; c < NEQ; ++c) U[c] = u[c * n + base + k];
+    const double m2 = NEQ == 4 ? U[1] * U[1] + U[2] * U[2] : U[1] * U[1];
+    const double pk = g1 * (U[NEQ - 1] - 0.5 * m2 / U[0]);
+    if (pk >= ep) continue;
+    double d[NEQ];
+    for (int c = 0; c < NEQ; ++c) d[c] = U[c] - mean[c];
+    const double dm2 = NEQ == 4 ? d[1] * d[1] + d[2] * d[2] : d[1] * d[1];
+    const double mdm = NEQ == 4 ? mean[1] * d[1] + mean[2] * d[2] : mean[1] * d[1];
+    // rho(t) (p(t) - eps_p) = a t^2 + b t + c along mean + t d
+    const double a = g1 * (d[NEQ - 1] * d[0] - 0.5 * dm2);
+    const double b = g1 * (mean[NEQ - 1] * d[0] + mean[0] * d[NEQ - 1] - mdm) - ep * d[0];
+    const double cc = mean[0] * (pbar - ep);
+    theta = fmin(theta, root01(a, b, cc));
+  }
+  if (theta < 1.0)
+    for (int k = 0; k < npts; ++k)
+      for (int c = 0; c < NEQ; ++c) {
+        double& v = u[c * n + base + k];
+        v = mean[c] + theta * (v - mean[c]);
+      }
+}
+
+// one thread per element; `force` ignores the step's completion flag
+__global__ void zs_limiter_2d(double* u, const Mesh2Dev M, Weights W, int np, double g1, double er, double ep,
+                              DevScalars* sc, int force) {
+  if (!force && !(sc && sc->stepped_ok)) return;
+  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;  // the prime pass recomputes it
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  if (M.solid && M.solid[e]) return;
+  const int np2 = np * np;
+  const size_t n = (size_t)M.nel * np2, base = (size_t)e * np2;
+  double ww[kMaxNp * kMaxNp];
+  const int gx = e % M.nx, gy = e / M.nx;
+  for (int k = 0; k < np2; ++k) {
+    const double absJ = M.curved ? fabs(1.0 / M.m_rJ[base + k]) : fabs(M.Jx[gx] * M.Jy[gy]);
+    ww[k] = W.w[k % np] * W.w[k / np] * absJ;
+  }
+  zs_element<4>(u, n, base, np2, ww, g1, er, ep);
+}
+
+__global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, double g1, double er, double ep,
+                              DevScalars* sc, int force) {
+  if (!force && !(sc && sc->stepped_ok)) return;
+  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  const size_t n = (size_t)M.nel * np, base = (size_t)e * np;
+  double ww[kMaxNp];
+  for (int k = 0; k < np; ++k) ww[k] = W.w[k] * M.J[e];
+  zs_element<3>(u, n, base, np, ww, g1, er, ep);
+}
+
+}  // namespace
+
+// Enqueue the post-step hook of a solve on its stream (no-op without one):
+// the hook kernel, then the prime pass of the limited state.  force: run even
+// if no step just completed.
+int enqueue_post_step(frg_solve* s, bool force) {
+  if (s->post_step_id != kHookPositivity) return FRG_OK;
+  Weights W;
+  std::memset(&W, 0, sizeof(W));
+  for (int i = 0; i < s->np; ++i) W.w[i] = s->ops.w[i];
+  const int threads = 128, blocks = (s->nel + threads - 1) / threads;
+  const double er = s->post_step_params[0], ep = s->post_step_params[1];
+  cudaStream_t st = s->ctx->stream;
+  if (s->dim == 2)
+    zs_limiter_2d<<<blocks, threads, 0, st>>>(s->U[0], s->L2.mesh, W, s->np, s->L2.phys.g1, er, ep, s->sc,
+                                               force ? 1 : 0);
+  else
+    zs_limiter_1d<<<blocks, threads, 0, st>>>(s->U[0], s->L1.mesh, W, s->np, s->L1.phys.g1, er, ep, s->sc,
+                                               force ? 1 : 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return rt::cuda_err(s->ctx, e, "post-step hook");
+  return rt::prime(s, 0, true);
+}
+
+}  // namespace frg
+
+using namespace frg;
+using namespace frg::rt;
+
+extern "C" {
+
+int frg_hook_count(void) { return kNumHooks; }
+
+int frg_hook_info(int i, const char** name, int* slot, int* id, int* nparams) {
+  if (i < 0 || i >= kNumHooks) return FRG_ERR_INVALID_ARG;
+  if (name) *name = kHooks[i].name;
+  if (slot) *slot = kHooks[i].slot;
+  if (id) *id = kHooks[i].id;
+  if (nparams) *nparams = kHooks[i].nparams;
+  return FRG_OK;
+}
+
+int frg_hook_lookup(const char* name, int* slot, int* id) {
+  if (!name) return FRG_ERR_INVALID_ARG;
+  for (int i = 0; i < kNumHooks; ++i)
+    if (std::strcmp(name, kHooks[i].name) == 0) {
+      if (slot) *slot = kHooks[i].slot;
+      if (id) *id = kHooks[i].id;
+      return FRG_OK;
+    }
+  return FRG_ERR_UNSUPPORTED_HOOK;
+}
+
+int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  if (slot != FRG_HOOK_POST_STEP) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook slot");
+  if (id == 0) {
+    s->post_step_id = 0;
+  } else {
+    int found = -1;
+    for (int i = 0; i < kNumHooks; ++i)
+      if (kHooks[i].slot == slot && kHooks[i].id == id) found = i;
+    if (found < 0) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook implementation");
+    if (nparams < 0 || nparams > kHooks[found].nparams || (nparams > 0 && !params))
+      return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters");
+    double p[2] = {1e-13, 1e-13};
+    for (int k = 0; k < nparams; ++k) p[k] = params[k];
+    if (!(p[0] > 0.0) || !(p[1] > 0.0)) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "eps_rho, eps_p must be > 0");
+    s->post_step_id = id;
+    s->post_step_params[0] = p[0];
+    s->post_step_params[1] = p[1];
+  }
+  // captured step graphs do not contain the hook (or contain the old one)
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  return FRG_OK;
+}
+
+int frg_apply_post_step(frg_solve* s) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  if (!s->have_state) return set_err(s->ctx, FRG_ERR_STATE, "no state uploaded");
+  cudaSetDevice(s->ctx->device);
+  int rc = make_current_canonical(s);
+  if (rc) return rc;
+  if ((rc = enqueue_post_step(s, true))) return rc;
+  return cuda_err(s->ctx, cudaStreamSynchronize(s->ctx->stream), "post-step hook");
+}
+
+}  // extern "C"

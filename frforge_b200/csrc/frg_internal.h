@@ -101,13 +101,16 @@ struct DevScalars {
   int active;                   // the step in flight runs
   int diverged_stage;           // 1..3, 4 = end-of-step state check
   int two_p1;                   // 2p+1
-  int pad;
+  int stepped_ok;               // the last step ran and did not diverge (post-step hooks)
   long long n_steps;
   long long max_steps;
   long long residual_evals;
 };
 
 enum : int { kRunning = 0, kFinished = 3 };
+
+// device hook implementations (frg_hooks.cu)
+enum : int { kHookNone = 0, kHookPositivity = 1 };
 
 // Stage kernel launch parameters (shared by the 1D and 2D kernels).
 struct StageBufs {

@@ -45,6 +45,8 @@ struct frg_solve {
   bool graph_lambda = false;
   int64_t residual_evals = 0, steps = 0;
   double hmin = 0.0;
+  int post_step_id = 0;  // device post-step hook (frg_hooks.cu), 0 = none
+  double post_step_params[2] = {0.0, 0.0};
 };
 
 
@@ -60,6 +62,8 @@ int finish_run(frg_solve* s);
 int make_current_canonical(frg_solve* s);
 void init_run_scalars(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps);
 }  // namespace rt
+// post-step hook of a solve and the prime pass of its result (frg_hooks.cu)
+int enqueue_post_step(frg_solve* s, bool force);
 __global__ void step_begin_kernel(DevScalars* sc);
 __global__ void step_end_kernel(DevScalars* sc, int nstages);
 }  // namespace frg

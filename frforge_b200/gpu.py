@@ -172,6 +172,24 @@ class GpuSolve:
         self.handle = h
         info = self.info()
         self.ndof, self.nel = info["ndof"], info["nel"]
+        # device implementations of the hooks the method overrides
+        for slot, (name, params) in (method or NullCapturing()).gpu_spec().get("hooks", {}).items():
+            self.set_hook(slot, name, params)
+
+    def set_hook(self, slot: str, name: str, params=()) -> None:
+        """Select the device implementation `name` of hook `slot`
+        ("post_step"); see frg_solve_set_hook."""
+        sl, hid = C.c_int(), C.c_int()
+        self._chk(L.load().frg_hook_lookup(name.encode(), C.byref(sl), C.byref(hid)), "frg_hook_lookup")
+        if sl.value != L.HOOK_SLOT[slot]:
+            raise ValueError(f"{name} implements another hook slot")
+        arr = np.ascontiguousarray(np.asarray(params, dtype=np.float64))
+        self._chk(L.load().frg_solve_set_hook(self.handle, sl.value, hid.value, L.dptr(arr) if arr.size else None,
+                                              int(arr.size)), "frg_solve_set_hook")
+
+    def apply_post_step(self) -> None:
+        """Run the post-step hook once on the current state."""
+        self._chk(L.load().frg_apply_post_step(self.handle), "frg_apply_post_step")
 
     def close(self):
         if getattr(self, "handle", None):
@@ -290,7 +308,8 @@ class GpuSolve:
 def _solve_for(state, eq, method, time=None) -> GpuSolve:
     method = method or NullCapturing()
     spec = method.gpu_spec()
-    key = (tuple(sorted(spec.items())), time or state.scheme.time, state.scheme, eq.gamma)
+    hooks = tuple(sorted(spec.pop("hooks", {}).items()))
+    key = (tuple(sorted(spec.items())), hooks, time or state.scheme.time, state.scheme, eq.gamma)
     s = state._gpu.get(key)
     if s is None:
         s = GpuSolve(state, eq, method, time=time)

@@ -54,12 +54,18 @@ class AbstractCapturingMethod:
         else:
             raise UnsupportedHookError(FRG_ERR_UNSUPPORTED_HOOK,
                                        f"{type(self).__name__} has no GPU implementation")
+        device = getattr(self, "gpu_hooks", {}) or {}
         for h in HOOKS:
             if getattr(type(self), h) is not getattr(known, h):
-                raise UnsupportedHookError(
-                    FRG_ERR_UNSUPPORTED_HOOK,
-                    f"{type(self).__name__}.{h} overrides a hook the GPU path cannot run")
-        return known._spec(self)
+                # an overridden hook runs on the GPU only if the method names a
+                # registered device implementation for it
+                if h.rstrip("_") not in device:
+                    raise UnsupportedHookError(
+                        FRG_ERR_UNSUPPORTED_HOOK,
+                        f"{type(self).__name__}.{h} overrides a hook the GPU path cannot run")
+        spec = known._spec(self)
+        spec["hooks"] = {slot: (name, tuple(params)) for slot, (name, params) in device.items()}
+        return spec
 
     @staticmethod
     def _spec(m) -> dict:
@@ -133,6 +139,31 @@ class ScaledPerssonMethod(AbstractCapturingMethod):
         return m.inner.gpu_spec()
 
 
+class PositivityPreservingPersson(PerssonAVMethod):
+    """Persson AV plus the Zhang-Shu positivity-preserving scaling after
+    every step: a capturing method that overrides post_step!
+    (Interfaces.jl:88-91) and names the device implementation of that hook,
+    so it runs on the GPU (frg_hooks.cu); post_step_ is the host
+    restatement (frforge_b200.limiters)."""
+
+    def __init__(self, kappa=4.0, s0_factor=-4.0, c_av=0.1, av_form="conservative_br0", eps_rho=1e-13,
+                 eps_p=1e-13):
+        super().__init__(kappa, s0_factor, c_av, av_form)
+        self.eps_rho, self.eps_p = float(eps_rho), float(eps_p)
+        self.gpu_hooks = {"post_step": ("positivity_zhang_shu", (self.eps_rho, self.eps_p))}
+
+    def post_step_(self, state, eq):
+        from .limiters import zhang_shu_limit_
+
+        zhang_shu_limit_(state, eq, self.eps_rho, self.eps_p)
+        return None
+
+    def method_params(self):
+        p = super().method_params()
+        p.update({"method": "persson_av_positive", "eps_rho": self.eps_rho, "eps_p": self.eps_p})
+        return p
+
+
 _GPU_CLASSES = (ScaledPerssonMethod, PerssonAVMethod, NullCapturing)
 
 # Method registry (Interfaces.jl:118-135, src/methods/Registry.jl:14-53)
@@ -140,6 +171,7 @@ METHOD_REGISTRY: Dict[str, Callable[..., AbstractCapturingMethod]] = {
     "null": lambda **kw: NullCapturing(),
     "persson_av": lambda **kw: PerssonAVMethod(**kw),
     "scaled_persson": lambda **kw: ScaledPerssonMethod(**kw),
+    "persson_av_positive": lambda **kw: PositivityPreservingPersson(**kw),
 }
 
 

@@ -15,6 +15,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _lib as L
+from .batch import _refuse_hooks
 from .gpu import Context, default_context, make_desc
 from .methods import AbstractCapturingMethod
 
@@ -52,6 +53,7 @@ class Server:
         """Queue ``integrate_(state, eq, method, t_final; cfl, dt, max_steps)``;
         returns the request id.  want_state=False: only the device-side
         diagnostics of the final state are returned, not the state."""
+        _refuse_hooks(method)
         d, keep = make_desc(state, eq, method, time)
         u0 = np.ascontiguousarray(np.asarray(state.u, dtype=np.float64).ravel(order="F"))
         out = np.empty_like(u0) if want_state else None
@@ -69,6 +71,7 @@ class Server:
         """As submit, with the initial state evaluated on the device at
         admission from the case IC ``ic`` (keyword arguments of
         frforge_b200._lib.make_ic); ``state`` gives the mesh and scheme only."""
+        _refuse_hooks(method)
         d, keep = make_desc(state, eq, method, time)
         c_ic = L.make_ic(**ic)
         out = np.empty(int(np.prod(state.u.shape))) if want_state else None

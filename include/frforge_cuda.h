@@ -389,6 +389,28 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
                          double cfl, double fixed_dt, int64_t max_steps, double* u_out,
                          int64_t* request_id);
 
+/* --------------------------------------------------------- device hooks
+   A registry of compiled implementations of capturing-method hooks, chosen
+   by name, so a method that overrides a hook can still run on the GPU
+   (no counterpart in the reference, whose hooks are Julia methods:
+   src/capturing/Interfaces.jl:43-92).  Slots: post_step (called after every
+   completed step, before the next compute_dt, as post_step! in
+   ssp_rk3_step!, SSP_RK3.jl:162).  Implementations:
+     "positivity_zhang_shu"  post_step: the positivity-preserving scaling of
+        Zhang & Shu (J. Comput. Phys. 229, 2010) toward the element mean,
+        density >= params[0], pressure >= params[1] (default 1e-13 each);
+        element integrals are unchanged.
+   Batched instances run no hooks (frg_batch_start refuses them). */
+enum { FRG_HOOK_POST_STEP = 0 };
+int frg_hook_count(void);
+int frg_hook_info(int index, const char** name, int* slot, int* id, int* nparams);
+/* FRG_ERR_UNSUPPORTED_HOOK if no implementation has that name. */
+int frg_hook_lookup(const char* name, int* slot, int* id);
+/* id 0 removes the slot's hook. */
+int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams);
+/* Apply the post-step hook once to the current state (host-driven loops). */
+int frg_apply_post_step(frg_solve* s);
+
 #ifdef __cplusplus
 }
 #endif
