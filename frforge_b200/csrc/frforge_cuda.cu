@@ -165,37 +165,30 @@ int prime(frg_solve* s, int buf, bool want_lambda) {
   return launch(s, b);
 }
 
-// The kernels of one time step on the current stream (RK3: 3 stages).
-// With `ev` (an array of 2*nstages events) each stage kernel is bracketed by
-// events for profiling.
-int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
-  step_begin_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc);
+// Stage buffers of SSP-RK stage `stage` of a solve (buffer rotation U0 ->
+// U1 -> U2 -> U0, SSP_RK3.jl:135-164 / SSP_RK2.jl:42-48).
+StageBufs stage_bufs(const frg_solve* s, int stage, bool want_lambda) {
   const bool rk2 = s->time_scheme == FRG_TIME_SSP_RK2;
   StageBufs b{};
   b.use_sc = 1;
   b.sc = s->sc;
   b.mode = kModeStage;
   b.rk2 = rk2;
-  // stage 1: u1 = u0 + dt L(u0)
-  b.stage = 1;
-  b.us = s->U[0];
+  b.stage = stage;
   b.u0 = s->U[0];
-  b.uout = s->U[1];
-  b.eps_in = s->E[0];
-  b.eps_out = s->E[1];
-  b.a = 1.0;
-  b.b = 0.0;
-  b.c = 1.0;
   b.want_lambda = 0;
-  if (ev) cudaEventRecord(ev[0], s->ctx->stream);
-  int rc = launch(s, b);
-  if (ev) cudaEventRecord(ev[1], s->ctx->stream);
-  if (rc) return rc;
-  if (rk2) {
-    // u = 1/2 u0 + 1/2 u1 + 1/2 dt L(u1)  (SSP_RK2.jl:42-48)
-    b.stage = 2;
+  if (stage == 1) {
+    // u1 = u0 + dt L(u0)
+    b.us = s->U[0];
+    b.uout = s->U[1];
+    b.eps_in = s->E[0];
+    b.eps_out = s->E[1];
+    b.a = 1.0;
+    b.b = 0.0;
+    b.c = 1.0;
+  } else if (rk2) {
+    // u = 1/2 u0 + 1/2 u1 + 1/2 dt L(u1)
     b.us = s->U[1];
-    b.u0 = s->U[0];
     b.uout = s->U[0];
     b.eps_in = s->E[1];
     b.eps_out = s->E[0];
@@ -203,29 +196,18 @@ int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
     b.b = 1.0 / 2.0;
     b.c = 1.0 / 2.0;
     b.want_lambda = want_lambda;
-    if (ev) cudaEventRecord(ev[2], s->ctx->stream);
-    rc = launch(s, b);
-    if (ev) cudaEventRecord(ev[3], s->ctx->stream);
-    if (rc) return rc;
-  } else {
+  } else if (stage == 2) {
     // u2 = 3/4 u0 + 1/4 u1 + 1/4 dt L(u1)
-    b.stage = 2;
     b.us = s->U[1];
-    b.u0 = s->U[0];
     b.uout = s->U[2];
     b.eps_in = s->E[1];
     b.eps_out = s->E[2];
     b.a = 3.0 / 4.0;
     b.b = 1.0 / 4.0;
     b.c = 1.0 / 4.0;
-    if (ev) cudaEventRecord(ev[2], s->ctx->stream);
-    rc = launch(s, b);
-    if (ev) cudaEventRecord(ev[3], s->ctx->stream);
-    if (rc) return rc;
+  } else {
     // u = 1/3 u0 + 2/3 u2 + 2/3 dt L(u2)
-    b.stage = 3;
     b.us = s->U[2];
-    b.u0 = s->U[0];
     b.uout = s->U[0];
     b.eps_in = s->E[2];
     b.eps_out = s->E[0];
@@ -233,9 +215,21 @@ int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
     b.b = 2.0 / 3.0;
     b.c = 2.0 / 3.0;
     b.want_lambda = want_lambda;
-    if (ev) cudaEventRecord(ev[4], s->ctx->stream);
-    rc = launch(s, b);
-    if (ev) cudaEventRecord(ev[5], s->ctx->stream);
+  }
+  return b;
+}
+
+// The kernels of one time step on the current stream (RK3: 3 stages).
+// With `ev` (an array of 2*nstages events) each stage kernel is bracketed by
+// events for profiling.
+int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
+  step_begin_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc);
+  const bool rk2 = s->time_scheme == FRG_TIME_SSP_RK2;
+  const int ns = rk2 ? 2 : 3;
+  for (int stage = 1; stage <= ns; ++stage) {
+    if (ev) cudaEventRecord(ev[2 * (stage - 1)], s->ctx->stream);
+    const int rc = launch(s, stage_bufs(s, stage, want_lambda));
+    if (ev) cudaEventRecord(ev[2 * (stage - 1) + 1], s->ctx->stream);
     if (rc) return rc;
   }
   step_end_kernel<<<1, 1, 0, s->ctx->stream>>>(s->sc, rk2 ? 2 : 3);

@@ -126,6 +126,9 @@ struct frg_batch {
   int* h_nrun = nullptr;  // pinned
   struct Group {
     int dim, np, flux, av, variant;
+    // solo: one instance large enough to fill the device by itself, stepped
+    // with the single-solve stage kernels (its own tuned tile shape)
+    bool solo = false;
     HostOps ops;  // the group's tables (copied: members come and go)
     std::vector<BatchTile> tiles;
     std::vector<int> members;
@@ -153,6 +156,9 @@ struct frg_batch {
 namespace {
 
 constexpr int kMaxReps = 32;  // multirate: most steps per round of one group
+// An instance with at least this many batched tiles (a full wave of resident
+// CTAs on 148 SMs) gains nothing from sharing launches and runs solo.
+constexpr int kSoloTiles = 600;
 
 int bcheck(frg_batch* b, cudaError_t e, const char* what) { return cuda_err(b->ctx, e, what); }
 
@@ -206,34 +212,47 @@ int rebuild(frg_batch* b) {
     const int av = s->dim == 2 ? s->L2.av : s->L1.av;
     const int flux = s->dim == 2 ? s->L2.flux : s->L1.flux;
     const int variant = 0;  // the batched kernels use one fixed tile shape per NP
-    frg_batch::Group* grp = nullptr;
-    for (auto& g : b->groups)
-      if (g.dim == s->dim && g.np == s->np && g.flux == flux && g.av == av && g.variant == variant &&
-          same_tables(g.ops, s->ops)) {
-        grp = &g;
-        break;
-      }
-    if (!grp) {
-      frg_batch::Group g;
-      g.dim = s->dim;
-      g.np = s->np;
-      g.flux = flux;
-      g.av = av;
-      g.variant = variant;
-      g.ops = s->ops;
-      b->groups.push_back(g);
-      grp = &b->groups.back();
-    }
     int tx = 1, ty = 1;
     batch_tile_shape(s->dim, s->np, variant, &tx, &ty);
+    // the choice depends on the instance alone, so its results do not
+    // depend on what else is in the batch
+    const bool solo = s->dim == 2 && (long)((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) >= kSoloTiles;
+    frg_batch::Group* grp = nullptr;
+    if (!solo)
+      for (auto& g : b->groups)
+        if (!g.solo && g.dim == s->dim && g.np == s->np && g.flux == flux && g.av == av && g.variant == variant &&
+            same_tables(g.ops, s->ops)) {
+          grp = &g;
+          break;
+        }
+    if (!grp)
+      for (auto& g : b->groups)  // reuse an emptied group's device buffer
+        if (g.members.empty()) {
+          grp = &g;
+          break;
+        }
+    if (!grp) {
+      b->groups.emplace_back();
+      grp = &b->groups.back();
+    }
+    if (grp->members.empty()) {
+      grp->dim = s->dim;
+      grp->np = s->np;
+      grp->flux = flux;
+      grp->av = av;
+      grp->variant = variant;
+      grp->solo = solo;
+      grp->ops = s->ops;
+    }
+    grp->members.push_back(i);
+    grp->ndof += s->ndof;
+    if (solo) continue;
     if (s->dim == 2) {
       for (int y = 0; y < s->ny; y += ty)
         for (int x = 0; x < s->nx; x += tx) grp->tiles.push_back(BatchTile{i, x, y, 0});
     } else {
       for (int x = 0; x < s->nx; x += tx) grp->tiles.push_back(BatchTile{i, x, 0, 0});
     }
-    grp->members.push_back(i);
-    grp->ndof += s->ndof;
   }
   // drop empty groups, upload tile and member lists
   b->groups.erase(std::remove_if(b->groups.begin(), b->groups.end(),
@@ -279,6 +298,16 @@ int enqueue_group_step(frg_batch* b, const frg_batch::Group& g, cudaStream_t st)
   const int m = (int)g.members.size();
   const int nb = (m + 127) / 128;
   batch_begin_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
+  if (g.solo) {
+    const frg_solve* s = b->slot[g.members[0]];
+    const int ns = s->time_scheme == FRG_TIME_SSP_RK2 ? 2 : 3;
+    for (int stage = 1; stage <= ns; ++stage) {
+      const int e = launch_stage2d(s->L2, stage_bufs(s, stage, true), st);
+      if (e) return bcheck(b, (cudaError_t)e, "solo stage launch");
+    }
+    batch_end_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
+    return bcheck(b, cudaGetLastError(), "batch control kernels");
+  }
   for (int stage = 1; stage <= 3; ++stage) {
     const int e = g.dim == 2 ? launch_batch2d(&g.ops, g.flux, g.av, g.variant, b->d_insts, g.d_tiles(),
                                               (int)g.tiles.size(), stage, kModeStage, st)

@@ -61,6 +61,7 @@ int prime(frg_solve* s, int buf, bool want_lambda);
 int finish_run(frg_solve* s);
 int make_current_canonical(frg_solve* s);
 void init_run_scalars(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps);
+StageBufs stage_bufs(const frg_solve* s, int stage, bool want_lambda);
 }  // namespace rt
 // post-step hook of a solve and the prime pass of its result (frg_hooks.cu)
 int enqueue_post_step(frg_solve* s, bool force);

@@ -9,6 +9,9 @@
   the two kernels read the mesh and stage descriptors from different memory
   (shared memory vs kernel parameters), so the compiler fuses a few
   multiply-adds differently.
+* Instances large enough to fill the device alone (a full wave of batched
+  tiles) run solo inside the batch, through the single-solve stage kernels:
+  they end bit-identical to the single-solve path.
 * One batched instance is checked against the oracle directly."""
 import numpy as np
 import pytest
@@ -140,6 +143,38 @@ def test_batch_mix_matches_solo_bitwise_and_single_path():
         _close(u, u_one)
     # empty slots report None
     assert all(res[k] is None for k in range(len(items), len(items) + 3))
+    b.close()
+
+
+def test_large_instances_run_solo_bitwise_equal_to_single_path():
+    # 200^2 P=3 RK3 (1,250 batched tiles) and 200^2 P=2 RK2 (850) run solo;
+    # the 12^2 instance is batched beside them
+    cases = [
+        (dict(dim=2, p=3, nx=200, ny=200, flux="hllc", method="persson", bcs=("transmissive",) * 4), "quad",
+         dict(t_final=1.0, cfl=0.1, max_steps=6)),
+        (dict(dim=2, p=2, nx=200, ny=200, flux="rusanov", time="ssp_rk2", method="persson"), "smooth",
+         dict(t_final=1.0, cfl=0.1, max_steps=5)),
+        (dict(dim=2, p=3, nx=12, ny=12, flux="hllc", method="persson", bcs=("transmissive",) * 4), "quad",
+         dict(t_final=1.0, cfl=0.1, max_steps=9)),
+    ]
+    items = _setup(cases, seed0=40)
+    single = [_run_alone(solve, u0, run) for (_, _, solve, u0, run, _) in items]
+    solo_small = _solo(items[2][1], items[2][5], items[2][4])
+    b = Batch(capacity=3)
+    slots = []
+    for (orc, state, solve, u0, run, kw) in items:
+        i = b.add(state, _eq(kw), _method(kw))
+        b.start(i, run["t_final"], cfl=run.get("cfl", 0.2), dt=run.get("dt"), max_steps=run["max_steps"])
+        slots.append(i)
+    res = b.run()
+    for k in (0, 1):
+        u, t = b.download(slots[k])
+        r_one, u_one, t_one = single[k]
+        assert res[slots[k]]["status"] == r_one["status"] == "max_steps", k
+        assert res[slots[k]]["n_steps"] == r_one["n_steps"], k
+        assert t == t_one and np.array_equal(u, u_one), k
+    u, t = b.download(slots[2])
+    assert res[slots[2]] == solo_small[0] and t == solo_small[2] and np.array_equal(u, solo_small[1])
     b.close()
 
 
