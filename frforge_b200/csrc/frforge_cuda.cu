@@ -336,16 +336,18 @@ int setup_2d(frg_solve* s, const frg_solve_desc* d) {
     std::memcpy(yv.data(), d->y_vertices, sizeof(double) * (ny + 1));
   else
     julia_linspace(d->y_bottom, d->y_top, ny + 1, yv.data());
-  std::vector<double> xc(nx), Jx(nx), dx(nx), yc(ny), Jy(ny), dy(ny), hchar(nel);
+  std::vector<double> xc(nx), Jx(nx), dx(nx), rJx(nx), yc(ny), Jy(ny), dy(ny), rJy(ny), hchar(nel);
   for (int i = 0; i < nx; ++i) {
     xc[i] = (xv[i] + xv[i + 1]) / 2.0;
     dx[i] = xv[i + 1] - xv[i];
     Jx[i] = dx[i] / 2.0;
+    rJx[i] = 1.0 / Jx[i];
   }
   for (int i = 0; i < ny; ++i) {
     yc[i] = (yv[i] + yv[i + 1]) / 2.0;
     dy[i] = yv[i + 1] - yv[i];
     Jy[i] = dy[i] / 2.0;
+    rJy[i] = 1.0 / Jy[i];
   }
   for (int e = 0; e < nel; ++e) hchar[e] = std::fmin(dx[e % nx], dy[e / nx]);
   Mesh2Dev& M = s->L2.mesh;
@@ -364,14 +366,14 @@ int setup_2d(frg_solve* s, const frg_solve_desc* d) {
   M.xc = p;
   if ((rc = dev_upload(s, &p, Jx.data(), nx))) return rc;
   M.Jx = p;
-  if ((rc = dev_upload(s, &p, dx.data(), nx))) return rc;
-  M.dx = p;
+  if ((rc = dev_upload(s, &p, rJx.data(), nx))) return rc;
+  M.rJx = p;
   if ((rc = dev_upload(s, &p, yc.data(), ny))) return rc;
   M.yc = p;
   if ((rc = dev_upload(s, &p, Jy.data(), ny))) return rc;
   M.Jy = p;
-  if ((rc = dev_upload(s, &p, dy.data(), ny))) return rc;
-  M.dy = p;
+  if ((rc = dev_upload(s, &p, rJy.data(), ny))) return rc;
+  M.rJy = p;
   if (d->solid) {
     unsigned char* q;
     if ((rc = dev_upload(s, &q, d->solid, (size_t)nel))) return rc;

@@ -56,11 +56,11 @@ struct Mesh2Dev {
   int nx, ny, nel;
   int px, py;  // periodic in x / y
   const double* xc;  // [nx] column centres (xL+xR)/2
-  const double* Jx;  // [nx] dx/2
-  const double* dx;  // [nx]
+  const double* Jx;   // [nx] dx/2
+  const double* rJx;  // [nx] 1/Jx
   const double* yc;
   const double* Jy;
-  const double* dy;
+  const double* rJy;  // [ny] 1/Jy
   const double* hchar;  // [nel]
   int curved;
   const double* m_xxi;  // [nel*np2] per SP, element-major

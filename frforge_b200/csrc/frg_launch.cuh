@@ -61,12 +61,13 @@ FRG_V(3, 1, 8, 3, 3, false)
 FRG_V(3, 2, 4, 4, 4, false)
 template <>
 struct Variants2D<4> {
-  static constexpr int n = 3, batch = 0;
+  static constexpr int n = 4, batch = 0;
   template <int V> struct V_;
 };
 FRG_V(4, 0, 8, 2, 4, false)
 FRG_V(4, 1, 8, 3, 3, false)
 FRG_V(4, 2, 8, 4, 2, true)
+FRG_V(4, 3, 4, 4, 4, false)
 template <>
 struct Variants2D<5> {
   static constexpr int n = 2, batch = 0;
@@ -108,6 +109,9 @@ int launch2d_inst(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
       break;
     case 2:
       if constexpr (Variants2D<NP>::n > 2) return launch2d_var<NP, FLUX, AV, 2>(L, b, st);
+      break;
+    case 3:
+      if constexpr (Variants2D<NP>::n > 3) return launch2d_var<NP, FLUX, AV, 3>(L, b, st);
       break;
     default:
       break;

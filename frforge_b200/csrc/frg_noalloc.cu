@@ -39,8 +39,8 @@ constexpr int kNaMaxEl = FRG_NOALLOC_MAX_ELEMENTS;
 constexpr int kNaMaxSide = FRG_NOALLOC_MAX_SIDE;
 constexpr size_t kNaEps = 0;                            // [kNaMaxEl] eps
 constexpr size_t kNaHchar = kNaEps + kNaMaxEl;          // [kNaMaxEl] h_char
-constexpr size_t kNaCols = kNaHchar + kNaMaxEl;         // 3 x [kNaMaxSide]: xc, Jx, dx
-constexpr size_t kNaRows = kNaCols + 3 * kNaMaxSide;    // 3 x [kNaMaxSide]: yc, Jy, dy
+constexpr size_t kNaCols = kNaHchar + kNaMaxEl;         // 3 x [kNaMaxSide]: xc, Jx, 1/Jx
+constexpr size_t kNaRows = kNaCols + 3 * kNaMaxSide;    // 3 x [kNaMaxSide]: yc, Jy, 1/Jy
 constexpr size_t kNaScalars = kNaRows + 3 * kNaMaxSide;  // DevScalars
 constexpr size_t kNaDoubles = kNaScalars + (sizeof(DevScalars) + 7) / 8;
 
@@ -108,16 +108,16 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
     julia_linspace(d->y_bottom, d->y_top, ny + 1, h.yv);
   for (int i = 0; i < nx; ++i) {
     h.cols[i] = (h.xv[i] + h.xv[i + 1]) / 2.0;
-    h.cols[2 * kNaMaxSide + i] = h.xv[i + 1] - h.xv[i];
-    h.cols[kNaMaxSide + i] = h.cols[2 * kNaMaxSide + i] / 2.0;
+    h.cols[kNaMaxSide + i] = (h.xv[i + 1] - h.xv[i]) / 2.0;
+    h.cols[2 * kNaMaxSide + i] = 1.0 / h.cols[kNaMaxSide + i];
   }
   for (int i = 0; i < ny; ++i) {
     h.rows[i] = (h.yv[i] + h.yv[i + 1]) / 2.0;
-    h.rows[2 * kNaMaxSide + i] = h.yv[i + 1] - h.yv[i];
-    h.rows[kNaMaxSide + i] = h.rows[2 * kNaMaxSide + i] / 2.0;
+    h.rows[kNaMaxSide + i] = (h.yv[i + 1] - h.yv[i]) / 2.0;
+    h.rows[2 * kNaMaxSide + i] = 1.0 / h.rows[kNaMaxSide + i];
   }
   for (int e = 0; e < nel; ++e)
-    h.hchar[e] = std::fmin(h.cols[2 * kNaMaxSide + e % nx], h.rows[2 * kNaMaxSide + e / nx]);
+    h.hchar[e] = std::fmin(h.xv[e % nx + 1] - h.xv[e % nx], h.yv[e / nx + 1] - h.yv[e / nx]);
   DevScalars sc;
   std::memset(&sc, 0, sizeof(sc));
   sc.t = t;
@@ -142,10 +142,10 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
   M.py = d->bc[2].kind == FRG_BC_PERIODIC;
   M.xc = base + kNaCols;
   M.Jx = base + kNaCols + kNaMaxSide;
-  M.dx = base + kNaCols + 2 * kNaMaxSide;
+  M.rJx = base + kNaCols + 2 * kNaMaxSide;
   M.yc = base + kNaRows;
   M.Jy = base + kNaRows + kNaMaxSide;
-  M.dy = base + kNaRows + 2 * kNaMaxSide;
+  M.rJy = base + kNaRows + 2 * kNaMaxSide;
   M.hchar = base + kNaHchar;
   for (int k = 0; k < 4; ++k) {
     const frg_bc& b = d->bc[k];

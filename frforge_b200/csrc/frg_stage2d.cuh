@@ -4,8 +4,8 @@
 // one-element halo ring (no corners) of the stage input in shared memory.
 // Everything a stage needs happens on chip:
 //   P0  cp.async copies of the tile: u_s (tile + halo), the step-start state
-//       u0 of the tile and the per-slot mesh values (eps, Jx, Jy, dx, dy,
-//       h_char)
+//       u0 of the tile and the per-slot mesh values (eps, Jx, Jy, 1/Jx,
+//       1/Jy, h_char); every other per-element factor is a product of these
 //   P1  physical fluxes -> contravariant F~, G~ at every own solution point
 //       (Residual2D.jl:342-352)
 //   P2  every face point of the tile once: u traces of both sides
@@ -77,7 +77,7 @@ struct Smem2D {
   static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
   static constexpr int FS = odd_up(NP * 8);     // face stride: NP points x (fhat[4], ghat[4])
   // one tile buffer (doubles): u_s of tile + halo, u0 of the tile, per-slot
-  // raw mesh values [6][NSLOT] = eps, Jx, Jy, dx, dy, h_char
+  // mesh values [6][NSLOT] = eps, Jx, Jy, 1/Jx, 1/Jy, h_char
   static constexpr int bU = 0;
   static constexpr int bU0 = bU + NSLOT * ES;
   static constexpr int bRaw = bU0 + (U0S ? NOWN * ES : 0);
@@ -86,10 +86,7 @@ struct Smem2D {
   static constexpr int oG = oF + NOWN * ES;         // [NOWN][ES]
   static constexpr int oFV = oG + NOWN * ES;        // [NFV][FS]
   static constexpr int oFH = oFV + NFV * FS;        // [NFH][FS]
-  // per-slot factors of P2-P4: 1/(Jx Jy), eps/Jx^2, eps/Jy^2, 1/Jx, 1/Jy,
-  // eps/Jx, eps/Jy
-  static constexpr int oDer = oFH + NFH * FS;       // [7][NSLOT]
-  static constexpr int oRed = oDer + 7 * NSLOT;     // reduction scratch
+  static constexpr int oRed = oFH + NFH * FS;       // reduction scratch
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2 + 8;  // element ids, flags
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
@@ -186,6 +183,7 @@ FRG_DEV void tile_slots(const Mesh2Dev& M, const TileBuf& tb, const int tx0, con
         if (ownpos && !wrap) fl |= kSlotOwn;
         if (wrap) fl |= kSlotWrap;
         if (prime && !(fl & kSlotOwn)) el = -1;  // prime/sense: own elements only
+        if (el >= 0 && M.solid && M.solid[el]) fl |= kSlotSolid;
       }
     }
     tb.el[s] = el;
@@ -236,8 +234,8 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
     if (AV != kAvNone && !c.prime) cp_async8(&tb.raw[s], &B.eps_in[el]);
     cp_async8(&tb.raw[NSLOT + s], &M.Jx[gx]);
     cp_async8(&tb.raw[2 * NSLOT + s], &M.Jy[gy]);
-    cp_async8(&tb.raw[3 * NSLOT + s], &M.dx[gx]);
-    cp_async8(&tb.raw[4 * NSLOT + s], &M.dy[gy]);
+    cp_async8(&tb.raw[3 * NSLOT + s], &M.rJx[gx]);
+    cp_async8(&tb.raw[4 * NSLOT + s], &M.rJy[gy]);
     if (AV != kAvNone && (tb.flag[s] & kSlotOwn)) cp_async8(&tb.raw[5 * NSLOT + s], &M.hchar[el]);
   }
   cp_async_commit();
@@ -264,20 +262,13 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   const double* sEps = tb.raw;
   const double* sJx = tb.raw + NSLOT;
   const double* sJy = tb.raw + 2 * NSLOT;
-  const double* sDx = tb.raw + 3 * NSLOT;
-  const double* sDy = tb.raw + 4 * NSLOT;
+  const double* sRjx = tb.raw + 3 * NSLOT;  // 1/Jx
+  const double* sRjy = tb.raw + 4 * NSLOT;  // 1/Jy
   const double* sHc = tb.raw + 5 * NSLOT;
   double* sF = smem + S::oF;
   double* sG = smem + S::oG;
   double* sFV = smem + S::oFV;
   double* sFH = smem + S::oFH;
-  double* sRJ = smem + S::oDer;     // 1/(Jx Jy)
-  double* sEvx = sRJ + NSLOT;       // eps/Jx^2
-  double* sEvy = sEvx + NSLOT;      // eps/Jy^2
-  double* sRjx = sEvy + NSLOT;      // 1/Jx
-  double* sRjy = sRjx + NSLOT;      // 1/Jy
-  double* sEpsJx = sRjy + NSLOT;    // eps/Jx
-  double* sEpsJy = sEpsJx + NSLOT;  // eps/Jy
   double* sRed = smem + S::oRed;
 
   const int tid = threadIdx.x;
@@ -287,31 +278,6 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   const double dt = ctl.dt, tstage = ctl.tstage;
 
   cp_async_wait<WAIT>();
-  __syncthreads();
-  // per-element factors, once per slot instead of once per line or point;
-  // one factor per thread
-  {
-    constexpr int NV = kBR0 ? 7 : (kAV ? 3 : 1);
-    for (int idx = tid; idx < NV * NSLOT; idx += NT) {
-      const int v = idx / NSLOT, s = idx % NSLOT;
-      const int el = sEl[s];
-      if (el < 0) continue;
-      const double jx = sJx[s], jy = sJy[s];
-      const double eps = (kAV && !prime) ? sEps[s] : 0.0;
-      double r;
-      switch (v) {
-        case 0: r = 1.0 / (jx * jy); break;
-        case 1: r = eps / (jx * jx); break;
-        case 2: r = eps / (jy * jy); break;
-        case 3: r = 1.0 / jx; break;
-        case 4: r = 1.0 / jy; break;
-        case 5: r = eps / jx; break;
-        default: r = eps / jy; break;
-      }
-      sRJ[v * NSLOT + s] = r;
-      if (v == 0 && M.solid && M.solid[el]) sFlag[s] |= kSlotSolid;
-    }
-  }
   __syncthreads();
 
   // wave speeds of the new state (P5 in a stage, P6 in prime / sense), in the
@@ -463,9 +429,11 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
         if (kBR0) {
-          const double sa = vert ? sEpsJx[sA] : sEpsJy[sA], sb = vert ? sEpsJx[sB] : sEpsJy[sB];
-          const double tau =
-              br0_tau(sEps[sA], sEps[sB], vert ? sDx[sA] : sDy[sA], vert ? sDx[sB] : sDy[sB], P.p);
+          // eps/J of both sides; element widths 2 J (exact)
+          const double sa = sEps[sA] * (vert ? sRjx[sA] : sRjy[sA]);
+          const double sb = sEps[sB] * (vert ? sRjx[sB] : sRjy[sB]);
+          const double tau = br0_tau(sEps[sA], sEps[sB], 2.0 * (vert ? sJx[sA] : sJy[sA]),
+                                     2.0 * (vert ? sJx[sB] : sJy[sB]), P.p);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c)
             gh[c] = 0.5 * (sa * gA[c] + sb * gB[c]) - tau * (uB[c] - uA[c]);
@@ -511,7 +479,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
         if (kBR0) {
-          const double sc = vert ? sEpsJx[s] : sEpsJy[s];
+          const double sc = sEps[s] * (vert ? sRjx[s] : sRjy[s]);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) gh[c] = sc * (haveB ? gB[c] : gA[c]);
         }
@@ -574,9 +542,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double fhE = fw[FS] - fc;
       const double ghW = kBR0 ? fw[4] : 0.0;
       const double ghE = kBR0 ? fw[FS + 4] : 0.0;
-      const double rJa = M.curved ? 0.0 : sRJ[s];
-      const double ev = kAV ? sEvx[s] : 0.0;
-      const double rjx = kBR0 ? sRjx[s] : 0.0;
+      const double rjx = sRjx[s];
+      const double rJa = M.curved ? 0.0 : rjx * sRjy[s];
+      const double ev = kAV ? (sEps[s] * rjx) * rjx : 0.0;
       const size_t mrow = (size_t)sEl[s] * NP2 + NP * j;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
@@ -629,9 +597,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double fhN = fs[TX * FS] - gc;
       const double ghS = kBR0 ? fs[4] : 0.0;
       const double ghN = kBR0 ? fs[TX * FS + 4] : 0.0;
-      const double rJa = M.curved ? 0.0 : sRJ[s];
-      const double ev = kAV ? sEvy[s] : 0.0;
-      const double rjy = kBR0 ? sRjy[s] : 0.0;
+      const double rjy = sRjy[s];
+      const double rJa = M.curved ? 0.0 : sRjx[s] * rjy;
+      const double ev = kAV ? (sEps[s] * rjy) * rjy : 0.0;
       const size_t mbase = (size_t)sEl[s] * NP2 + i;
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
