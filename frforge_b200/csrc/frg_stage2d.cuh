@@ -380,8 +380,29 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           gB[c] = sg;
         }
       }
+      // BR0 averaged viscous flux first, so that the g traces are dead
+      // before the numerical flux
+      if (kBR0) {
+        double gh[4];
+        if (eA >= 0 && eB >= 0) {
+          // eps/J of both sides; element widths 2 J (exact)
+          const double sa = sEps[sA] * (vert ? sRjx[sA] : sRjy[sA]);
+          const double sb = sEps[sB] * (vert ? sRjx[sB] : sRjy[sB]);
+          const double tau = br0_tau(sEps[sA], sEps[sB], 2.0 * (vert ? sJx[sA] : sJy[sA]),
+                                     2.0 * (vert ? sJx[sB] : sJy[sB]), P.p);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = 0.5 * (sa * gA[c] + sb * gB[c]) - tau * (uB[c] - uA[c]);
+        } else {
+          const bool haveB = eB >= 0;
+          const int s = haveB ? sB : sA;
+          const double sc = sEps[s] * (vert ? sRjx[s] : sRjy[s]);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) gh[c] = sc * (haveB ? gB[c] : gA[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) out[4 + c] = gh[c];
+      }
       double fh[4] = {0.0, 0.0, 0.0, 0.0};
-      double gh[4] = {0.0, 0.0, 0.0, 0.0};
       const int fE = vert ? 1 : 3, fW = vert ? 0 : 2;  // face slots E/N and W/S
       if (eA >= 0 && eB >= 0) {
         const bool solA = flA & kSlotSolid, solB = flB & kSlotSolid;
@@ -428,16 +449,6 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
-        if (kBR0) {
-          // eps/J of both sides; element widths 2 J (exact)
-          const double sa = sEps[sA] * (vert ? sRjx[sA] : sRjy[sA]);
-          const double sb = sEps[sB] * (vert ? sRjx[sB] : sRjy[sB]);
-          const double tau = br0_tau(sEps[sA], sEps[sB], 2.0 * (vert ? sJx[sA] : sJy[sA]),
-                                     2.0 * (vert ? sJx[sB] : sJy[sB]), P.p);
-#pragma unroll
-          for (int c = 0; c < NEQ; ++c)
-            gh[c] = 0.5 * (sa * gA[c] + sb * gB[c]) - tau * (uB[c] - uA[c]);
-        }
       } else {
         // domain boundary: A missing (left/bottom) or B missing (right/top)
         const bool haveB = eB >= 0;
@@ -478,17 +489,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
-        if (kBR0) {
-          const double sc = sEps[s] * (vert ? sRjx[s] : sRjy[s]);
-#pragma unroll
-          for (int c = 0; c < NEQ; ++c) gh[c] = sc * (haveB ? gB[c] : gA[c]);
-        }
       }
 #pragma unroll
-      for (int c = 0; c < NEQ; ++c) {
-        out[c] = fh[c];
-        out[4 + c] = gh[c];
-      }
+      for (int c = 0; c < NEQ; ++c) out[c] = fh[c];
     }
     __syncthreads();
 
