@@ -89,6 +89,7 @@ struct Smem2D {
   static constexpr int oRed = oFH + NFH * FS;       // reduction scratch
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2 + 8;  // element ids, flags
+  static_assert(NOWN <= 256, "the viscosity pass covers a tile with one pass of the block");
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
   // 1 KB reserved per CTA plus the batched kernels' static descriptors
   static_assert(MINB * (bytes + 1024 + kBatchStaticSmem) <= 228 * 1024,
@@ -659,7 +660,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
             const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : u0r[it][c]);
             const double un = (B.a * u0 + B.b * us) + cdt * du;
             B.uout[gi] = un;
-            sF[li] = un;
+            if (c == 0) sF[li] = un;  // the sensor reads the new density
             unv[c] = un;
             chk_u = fma(un, 0.0, chk_u);
           }
@@ -726,13 +727,16 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         }
       }
     }
-    if (B.want_lambda) {
-      // block max of the CFL wave speed (compute_dt), one atomic per tile
+    // The CFL wave speed (compute_dt) of the tile: with the viscosity pass
+    // below, the maximum over its elements' maxima (taken there); otherwise a
+    // block maximum of the points' wave speeds.  One atomic per tile or warp.
+    const bool lam_blk = B.want_lambda && !(kAV && B.mode != kModeSense);
+    if (lam_blk) {
       for (int off = 16; off > 0; off >>= 1) lmax = jmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
       if ((tid & 31) == 0) sRed[tid >> 5] = lmax;
     }
     __syncthreads();
-    if (B.want_lambda && tid < 32) {
+    if (lam_blk && tid < 32) {
       double v = (tid < (NT >> 5)) ? sRed[tid] : 0.0;
       for (int off = 16; off > 0; off >>= 1) v = jmax(v, __shfl_xor_sync(0xffffffffu, v, off));
       if (tid == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, v);
@@ -760,6 +764,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       sPart[o * PS + 2 * i + 1] = ehigh;
     }
     __syncthreads();
+    double lcta = 0.0;
     for (int o = tid; o < NOWN; o += NT) {
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!(sFlag[s] & kSlotOwn)) continue;
@@ -772,6 +777,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       }
 #pragma unroll
       for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * WS + k]);
+      lcta = jmax(lcta, lam);
       lam = jmax(lam, kEps);
       const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
       if (B.mode == kModeSense) {
@@ -781,6 +787,11 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       double ev = 0.0;
       if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (sHc[s] / (double)P.pm) * lam;
       B.eps_out[el] = ev;
+    }
+    // the warps that hold elements (NOWN <= NT)
+    if (B.want_lambda && B.mode != kModeSense && tid < ((NOWN + 31) & ~31)) {
+      for (int off = 16; off > 0; off >>= 1) lcta = jmax(lcta, __shfl_xor_sync(0xffffffffu, lcta, off));
+      if ((tid & 31) == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, lcta);
     }
   }
 }
