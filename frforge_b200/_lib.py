@@ -84,6 +84,19 @@ class frg_diagnostics(C.Structure):
                 ("pad", C.c_int), ("l2_error", C.c_double), ("t", C.c_double)]
 
 
+class frg_shock_params(C.Structure):
+    _fields_ = [("ref_min", C.c_double), ("ref_max", C.c_double), ("grad_frac", C.c_double),
+                ("window_sp", C.c_int), ("n_exclude", C.c_int), ("exclude", (C.c_double * 2) * 4)]
+
+
+class frg_shock_metrics(C.Structure):
+    _fields_ = [("shock_thickness", C.c_double), ("shock_index", C.c_int64), ("shock_x", C.c_double),
+                ("overshoot", C.c_double), ("overshoot_over", C.c_double), ("overshoot_under", C.c_double),
+                ("rho_min", C.c_double), ("rho_max", C.c_double), ("excess_dissipation", C.c_double),
+                ("l1_rel", C.c_double), ("n_samples", C.c_int64), ("has_reference", C.c_int),
+                ("pad", C.c_int)]
+
+
 class frg_ic(C.Structure):
     _fields_ = [("kind", C.c_int), ("pad", C.c_int), ("x0", C.c_double), ("y0", C.c_double),
                 ("amp", C.c_double), ("phase", C.c_double), ("t", C.c_double), ("prim", (C.c_double * 4) * 4)]
@@ -186,6 +199,8 @@ SIGNATURES = {
     "frg_server_take_completed": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int,
                                             C.POINTER(C.c_int)]),
     "frg_server_diagnostics": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(frg_diagnostics)]),
+    "frg_shock_metrics_1d": (C.c_int, [C.c_void_p, C.POINTER(frg_shock_params), _dp, C.c_void_p,
+                                       C.POINTER(frg_shock_metrics)]),
 }
 
 _lib = None

@@ -276,6 +276,40 @@ class GpuSolve:
         with a device pointer ref_ptr)."""
         return diagnostics_of(self.handle, self.ctx, exact, t_exact, c, ref_ptr, self.info()["neq"])
 
+    def shock_metrics(self, ref=None, ref_min: float = 0.125, ref_max: float = 1.0, grad_frac: float = 0.15,
+                      exclude=(), window_sp: int = 30) -> dict:
+        """1D shock-capturing scores of the current density on the device
+        (Metrics.jl: shock_thickness_sp, overshoot_metric, excess_dissipation
+        over smooth_region_mask, and the relative L1): ref is None, a density
+        array in x order (e.g. an exact solution at the solution points), or
+        another 1D GpuSolve on the same mesh (e.g. the NullCapturing run)."""
+        prm = L.frg_shock_params()
+        prm.ref_min, prm.ref_max, prm.grad_frac = float(ref_min), float(ref_max), float(grad_frac)
+        prm.window_sp = int(window_sp)
+        exclude = list(exclude)
+        if len(exclude) > 4:
+            raise ValueError("at most 4 excluded windows")
+        prm.n_exclude = len(exclude)
+        for k, (a, b) in enumerate(exclude):
+            prm.exclude[k][0], prm.exclude[k][1] = float(a), float(b)
+        out = L.frg_shock_metrics()
+        ref_arr, ref_solve = None, None
+        if isinstance(ref, GpuSolve):
+            ref_solve = ref.handle
+        elif ref is not None:
+            ref_arr = np.ascontiguousarray(np.asarray(ref, dtype=np.float64).ravel())
+            if ref_arr.size != self.nel * self.state_shape[0]:
+                raise ValueError("reference density must have one value per solution point")
+        self._chk(L.load().frg_shock_metrics_1d(self.handle, C.byref(prm),
+                                                L.dptr(ref_arr) if ref_arr is not None else None, ref_solve,
+                                                C.byref(out)), "frg_shock_metrics_1d")
+        has_ref = bool(out.has_reference)
+        return {"shock_thickness": out.shock_thickness, "shock_index": int(out.shock_index),
+                "shock_x": out.shock_x, "overshoot": out.overshoot, "overshoot_over": out.overshoot_over,
+                "overshoot_under": out.overshoot_under, "rho_min": out.rho_min, "rho_max": out.rho_max,
+                "excess_dissipation": out.excess_dissipation if has_ref else None,
+                "l1_rel": out.l1_rel if has_ref else None, "n_samples": int(out.n_samples)}
+
     def variant(self):
         """(current tile variant, number of variants) of the stage kernel."""
         v, n = C.c_int(), C.c_int()

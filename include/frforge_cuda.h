@@ -350,6 +350,45 @@ int frg_diagnostics_compute(frg_solve* s, int exact, const double* ref_dev, doub
    request completed successfully. */
 int frg_server_diagnostics(frg_server* s, int64_t request_id, frg_diagnostics* out);
 
+/* 1D shock-capturing scores of a solve's density on the device: the scoring
+   fields of the reference's discontinuous 1D case reports (Cases.jl:987-1021)
+   from src/verification/Metrics.jl, over the density samples in x order
+   (sample_solution_1d, :95-123):
+     shock_thickness   shock_thickness_sp(x, rho) (:138-200), in mean
+                       solution-point spacings; NaN as the reference
+     shock_index/_x    0-based sample index and x of the steepest gradient
+     overshoot*        overshoot_metric(rho_min, rho_max, ref_min, ref_max)
+                       (:81-87)
+     excess_dissipation  excess_dissipation(x, rho, ref; mask =
+                       smooth_region_mask(x, ref; grad_frac, exclude))
+                       (:208-255); NaN without a reference
+     l1_rel            sum|rho - ref| / (sum|ref| + 1e-30) (Cases.jl:1021)
+   The reference density is either ref_host (n_samples doubles, host memory,
+   x order) or the current state of ref_solve (a 1D solve on the same
+   samples, e.g. the NullCapturing run of the same case), or neither.
+   Indices and the thickness are exact; sums are reduced in a fixed order. */
+typedef struct frg_shock_params {
+  double ref_min, ref_max; /* overshoot bounds (Sod: 0.125, 1.0) */
+  double grad_frac;        /* smooth_region_mask gradient fraction */
+  int window_sp;           /* shock_thickness_sp window, 1..512 (reference: 30) */
+  int n_exclude;           /* excluded x windows of the mask, 0..4 */
+  double exclude[4][2];    /* [a, b] windows (closed) */
+} frg_shock_params;
+typedef struct frg_shock_metrics {
+  double shock_thickness;
+  int64_t shock_index;
+  double shock_x;
+  double overshoot, overshoot_over, overshoot_under;
+  double rho_min, rho_max;
+  double excess_dissipation;
+  double l1_rel;
+  int64_t n_samples;
+  int has_reference;
+  int pad;
+} frg_shock_metrics;
+int frg_shock_metrics_1d(frg_solve* s, const frg_shock_params* params, const double* ref_host,
+                         const frg_solve* ref_solve, frg_shock_metrics* out);
+
 /* ------------------------------------------------------ initial conditions
    set_initial_condition! (SolutionState.jl:59-73, SolutionState2D.jl:58-82)
    for the reference's case initial conditions, evaluated on the device at

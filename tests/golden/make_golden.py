@@ -7,7 +7,9 @@ build container, never on a GPU host):
 * test/test_2d.jl:316-321 -- isentropic-vortex L2 errors and observed order;
 * test/data/snapshot_fixture/{baseline,method}.json -- quant-suite case
   reports (1D smooth-order L2 errors, Sod and Shu-Osher step counts and
-  extrema) recorded by Julia 1.11.7;
+  extrema, and their scoring fields: shock thickness, overshoot, excess
+  dissipation, L1 against the exact or reference density) recorded by
+  Julia 1.11.7;
 * test/data/shu_osher_ref.csv -- the self-generated Shu-Osher density
   reference (p=1, Ne=200, c_av=0.5, CFL 0.1).
 
@@ -40,13 +42,15 @@ def main(ref_root: str) -> None:
         for c in d["cases"]:
             keep = {k: c[k] for k in ("name", "p", "capturing_method", "diverged", "nan_detected",
                                       "positivity_ok", "pass") if k in c}
-            for k in ("l2_errors", "mesh_sizes", "observed_orders", "n_elements", "t_final"):
+            for k in ("l2_errors", "mesh_sizes", "observed_orders", "n_elements", "t_final", "shock_thickness",
+                      "overshoot", "excess_dissipation", "l1_error_vs_reference"):
                 if k in c:
                     keep[k] = c[k]
             if "method_params" in c:
                 keep["method_params"] = c["method_params"]
             mt = c.get("metrics", {})
-            for k in ("n_steps", "u_min", "u_max", "mass_change", "dt_fixed", "cfl", "n_elements_list"):
+            for k in ("n_steps", "u_min", "u_max", "mass_change", "dt_fixed", "cfl", "n_elements_list",
+                      "excess_dissipation_vs_exact", "excess_dissipation_vs_null", "l1_density_vs_exact"):
                 if k in mt:
                     keep[k] = mt[k]
             cases[c["name"]] = keep
