@@ -172,7 +172,8 @@ def test_large_instances_run_solo_bitwise_equal_to_single_path():
         r_one, u_one, t_one = single[k]
         assert res[slots[k]]["status"] == r_one["status"] == "max_steps", k
         assert res[slots[k]]["n_steps"] == r_one["n_steps"], k
-        assert t == t_one and np.array_equal(u, u_one), k
+        assert t == t_one, k
+        assert np.array_equal(u, u_one), (k, int(np.sum(u != u_one)), float(np.max(np.abs(u - u_one))))
     u, t = b.download(slots[2])
     assert res[slots[2]] == solo_small[0] and t == solo_small[2] and np.array_equal(u, solo_small[1])
     b.close()
