@@ -161,14 +161,29 @@ def workload_config(args):
             "l2": "inputs larger than L2 (3 x 134 MB state buffers)", "parallelism": f"replicas{args.gpus}"}
 
 
-def traffic_per_launch():
-    """dram bytes per stage launch from the committed ncu summary, if any."""
+def _profile_summary():
     path = os.path.join(ROOT, "profiles", "stage2d_c3_traffic.json")
     if not os.path.exists(path):
-        return None
+        return {}
     with open(path) as f:
-        d = json.load(f)
-    return d.get("dram_bytes_per_launch_full_c3")
+        return json.load(f)
+
+
+def traffic_per_launch():
+    """dram bytes per stage launch from the committed ncu summary, if any."""
+    return _profile_summary().get("dram_bytes_per_launch_full_c3")
+
+
+def issue_limiter():
+    """The stage kernel's issue-side figures from the committed ncu summary:
+    what bounds it below the HBM roofline."""
+    d = _profile_summary().get("issue_256sq")
+    if not d:
+        return None
+    return {"kind": "fp64 issue / latency", "fp64_pipe_busy": d["sm__pipe_fp64_cycles_active_pct"] / 100.0,
+            "issue_active": d["smsp__issue_active_pct"] / 100.0,
+            "warp_instructions_per_dof": d["warp_instructions_per_dof"],
+            "source": "ncu, profiles/stage2d_c3_ncu.md"}
 
 
 def max_over_ranks(ms: float, world: int, device: str) -> float:
@@ -290,7 +305,8 @@ def run_ours(args):
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "stage_ms": [float(x) for x in stage_ms], "peak_kind": peak_kind,
                          "tile_variant": int(variant),
-                         "variant_ms": [float(x) for x in variant_ms]},
+                         "variant_ms": [float(x) for x in variant_ms],
+                         "limiter": issue_limiter()},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": args.steps * 5,
