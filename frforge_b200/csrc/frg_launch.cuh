@@ -32,18 +32,20 @@ OpsT<NP> make_ops(const HostOps& h) {
   return o;
 }
 
-// Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory).
+// Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory,
+// and for FRG_VT the threads per CTA, else 256).
 // Variant 0 is the default, the fastest measured on a B200 for large meshes
 // (P=3: 512^2, P=4/5: 384^2); the autotuner times all of them on the solve.
 // The batched kernels use variant `batch`.
 template <int NP>
 struct Variants2D;
-#define FRG_V(NPv, idx, tx, ty, minb, u0s)                                              \
+#define FRG_VT(NPv, idx, tx, ty, minb, u0s, nt)                                         \
   template <>                                                                             \
   struct Variants2D<NPv>::V_<idx> {                                                       \
-    static constexpr int TX = tx, TY = ty, MINB = minb;                                   \
+    static constexpr int TX = tx, TY = ty, MINB = minb, NT = nt;                          \
     static constexpr bool U0S = u0s;                                                      \
   };
+#define FRG_V(NPv, idx, tx, ty, minb, u0s) FRG_VT(NPv, idx, tx, ty, minb, u0s, kStageThreads)
 template <>
 struct Variants2D<2> {
   static constexpr int n = 2, batch = 1;
@@ -61,34 +63,38 @@ FRG_V(3, 1, 8, 3, 3, false)
 FRG_V(3, 2, 4, 4, 4, false)
 template <>
 struct Variants2D<4> {
-  static constexpr int n = 4, batch = 0;
+  static constexpr int n = 5, batch = 1;
   template <int V> struct V_;
 };
-FRG_V(4, 0, 8, 2, 4, false)
-FRG_V(4, 1, 8, 3, 3, false)
-FRG_V(4, 2, 8, 4, 2, true)
-FRG_V(4, 3, 4, 4, 4, false)
+FRG_VT(4, 0, 8, 4, 2, false, 512)
+FRG_V(4, 1, 8, 2, 4, false)
+FRG_V(4, 2, 8, 3, 3, false)
+FRG_V(4, 3, 8, 4, 2, true)
+FRG_V(4, 4, 4, 4, 4, false)
 template <>
 struct Variants2D<5> {
-  static constexpr int n = 2, batch = 0;
+  static constexpr int n = 3, batch = 1;
   template <int V> struct V_;
 };
-FRG_V(5, 0, 4, 3, 3, false)
-FRG_V(5, 1, 4, 4, 2, true)
+FRG_VT(5, 0, 8, 3, 2, false, 512)
+FRG_V(5, 1, 4, 3, 3, false)
+FRG_V(5, 2, 4, 4, 2, true)
 template <>
 struct Variants2D<6> {
-  static constexpr int n = 2, batch = 0;
+  static constexpr int n = 3, batch = 1;
   template <int V> struct V_;
 };
-FRG_V(6, 0, 3, 3, 3, false)
-FRG_V(6, 1, 4, 3, 2, true)
+FRG_VT(6, 0, 6, 3, 2, false, 512)
+FRG_V(6, 1, 3, 3, 3, false)
+FRG_V(6, 2, 4, 3, 2, true)
 #undef FRG_V
+#undef FRG_VT
 
 template <int NP, int FLUX, int AV, int V>
 int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
   using VV = typename Variants2D<NP>::template V_<V>;
-  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB>;
-  auto kern = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S>;
+  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB, VV::NT>;
+  auto kern = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT>;
   static bool configured = false;  // the attribute belongs to the function
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
@@ -96,7 +102,7 @@ int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
     configured = true;
   }
   dim3 grid((L.mesh.nx + VV::TX - 1) / VV::TX, (L.mesh.ny + VV::TY - 1) / VV::TY);
-  kern<<<grid, kStageThreads, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
+  kern<<<grid, VV::NT, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
   return (int)cudaGetLastError();
 }
 
@@ -112,6 +118,12 @@ int launch2d_inst(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
       break;
     case 3:
       if constexpr (Variants2D<NP>::n > 3) return launch2d_var<NP, FLUX, AV, 3>(L, b, st);
+      break;
+    case 4:
+      if constexpr (Variants2D<NP>::n > 4) return launch2d_var<NP, FLUX, AV, 4>(L, b, st);
+      break;
+    case 5:
+      if constexpr (Variants2D<NP>::n > 5) return launch2d_var<NP, FLUX, AV, 5>(L, b, st);
       break;
     default:
       break;
@@ -170,6 +182,7 @@ template <int NP, int FLUX, int AV, int V>
 int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles, int ntiles, int stage,
                 int mode, cudaStream_t st) {
   using VV = typename Variants2D<NP>::template V_<V>;
+  static_assert(VV::NT == kStageThreads, "the batched kernels run kStageThreads per CTA");
   using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB>;
   auto kern = stage2d_batch_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S>;
   static bool configured = false;

@@ -69,8 +69,9 @@ constexpr int odd_up(int n) { return (n % 2) ? n : n + 1; }
 
 // Shared-memory layout.  U0S: stage the step-start state u0 in shared memory
 // (copied with the tile); otherwise the epilogue reads it from global memory.
-template <int NP, int TX, int TY, bool U0S = true, int MINB = 2>
+template <int NP, int TX, int TY, bool U0S = true, int MINB = 2, int NTHR = 256>
 struct Smem2D {
+  static constexpr int NT = NTHR;  // threads per CTA
   static constexpr int NEQ = 4, NP2 = NP * NP;
   static constexpr int BX = TX + 2, BY = TY + 2, NSLOT = BX * BY, NOWN = TX * TY;
   static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
@@ -89,7 +90,7 @@ struct Smem2D {
   static constexpr int oRed = oFH + NFH * FS;       // reduction scratch
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2 + 8;  // element ids, flags
-  static_assert(NOWN <= 256, "the viscosity pass covers a tile with one pass of the block");
+  static_assert(NOWN <= NTHR, "the viscosity pass covers a tile with one pass of the block");
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
   // 1 KB reserved per CTA plus the batched kernels' static descriptors
   static_assert(MINB * (bytes + 1024 + kBatchStaticSmem) <= 228 * 1024,
@@ -161,7 +162,7 @@ template <class S>
 FRG_DEV void tile_slots(const Mesh2Dev& M, const TileBuf& tb, const int tx0, const int ty0, const bool prime) {
   constexpr int BX = S::BX, BY = S::BY, NSLOT = S::NSLOT, TX = S::BX - 2, TY = S::BY - 2;
   const int nx = M.nx, ny = M.ny;
-  for (int s = threadIdx.x; s < NSLOT; s += kStageThreads) {
+  for (int s = threadIdx.x; s < NSLOT; s += S::NT) {
     const int bx = s % BX, by = s / BX;
     const bool corner = (bx == 0 || bx == BX - 1) && (by == 0 || by == BY - 1);
     int gx = tx0 + bx - 1, gy = ty0 + by - 1;
@@ -198,7 +199,7 @@ template <int NP, int AV, class S>
 FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb, const StageCtl& c) {
   constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, BX = S::BX, BY = S::BY, NSLOT = S::NSLOT;
   constexpr int TX = BX - 2, TY = BY - 2;
-  constexpr int NT = kStageThreads;
+  constexpr int NT = S::NT;
   constexpr bool U0S = (S::bRaw != S::bU0);
   const int tid = threadIdx.x;
   const size_t cs = (size_t)M.nel * NP2;  // component stride
@@ -251,7 +252,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
   constexpr int BX = S::BX, NSLOT = S::NSLOT, NOWN = S::NOWN;
   constexpr int TX = S::BX - 2, TY = S::BY - 2;
   constexpr int NFV = S::NFV, NFH = S::NFH;
-  constexpr int NT = kStageThreads;
+  constexpr int NT = S::NT;
   constexpr bool kBR0 = (AV == kAvBR0);
   constexpr bool kAV = (AV != kAvNone);
   constexpr bool U0S = (S::bRaw != S::bU0);
@@ -798,10 +799,10 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 
 // One tile of one stage (single buffer).  tx0, ty0: first element of the
 // tile.  Used by stage2d_kernel and by the batched kernels.
-template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S>
+template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S, int NTHR = kStageThreads>
 __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
                                              const StageBufs& B, const int tx0, const int ty0) {
-  using S = Smem2D<NP, TX, TY, U0S, MINB>;
+  using S = Smem2D<NP, TX, TY, U0S, MINB, NTHR>;
   extern __shared__ __align__(16) double smem[];
   StageCtl ctl;
   if (!stage_control(B, ctl)) return;
@@ -814,10 +815,10 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
 
 // Single solve, one tile per CTA: the grid covers the mesh with tiles.
 template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
-          bool U0S = true>
-__global__ void __launch_bounds__(kStageThreads, MINB)
+          bool U0S = true, int NTHR = kStageThreads>
+__global__ void __launch_bounds__(NTHR, MINB)
     stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
-  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
+  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
 }
 
 }  // namespace frg
