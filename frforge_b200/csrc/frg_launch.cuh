@@ -94,13 +94,17 @@ template <int NP, int FLUX, int AV, int V>
 int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
   using VV = typename Variants2D<NP>::template V_<V>;
   using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB, VV::NT>;
-  auto kern = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT>;
-  static bool configured = false;  // the attribute belongs to the function
+  // affine and curved meshes have kernels of their own
+  auto kaff = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT, 0>;
+  auto kcur = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT, 1>;
+  static bool configured = false;  // the attribute belongs to the functions
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    cudaError_t e = cudaFuncSetAttribute(kaff, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kcur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
     if (e != cudaSuccess) return (int)e;
     configured = true;
   }
+  auto kern = L.mesh.curved ? kcur : kaff;
   dim3 grid((L.mesh.nx + VV::TX - 1) / VV::TX, (L.mesh.ny + VV::TY - 1) / VV::TY);
   kern<<<grid, VV::NT, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
   return (int)cudaGetLastError();

@@ -245,9 +245,11 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
 
 // P1-P6 of one tile whose copies are in tb.  WAIT: cp.async groups that may
 // still be pending when the tile starts.
-template <int NP, int FLUX, int AV, class S, int WAIT>
+// CURV: 0 affine mesh, 1 curved mesh, -1 read from the descriptor.
+template <int NP, int FLUX, int AV, class S, int WAIT, int CURV = -1>
 FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P, const StageBufs& B,
                           const TileBuf& tb, double* smem, const StageCtl& ctl) {
+  const bool curved = CURV < 0 ? (M.curved != 0) : (CURV == 1);
   constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
   constexpr int BX = S::BX, NSLOT = S::NSLOT, NOWN = S::NOWN;
   constexpr int TX = S::BX - 2, TY = S::BY - 2;
@@ -302,7 +304,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       flux_xy(P.g1, U, F, G);
       double* fo = sF + o * ES + k;
       double* go = sG + o * ES + k;
-      if (M.curved) {
+      if (curved) {
         const size_t m = (size_t)sEl[s] * NP2 + k;
         const double xxi = M.m_xxi[m], xeta = M.m_xeta[m], yxi = M.m_yxi[m], yeta = M.m_yeta[m];
 #pragma unroll
@@ -418,7 +420,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           const int e = fluidB ? eB : eA;
           const int face = fluidB ? fW : fE;
           double nxo, nyo, sJ;
-          if (M.curved) {
+          if (curved) {
             nxo = M.f_nx[face][(size_t)e * NP + q];
             nyo = M.f_ny[face][(size_t)e * NP + q];
             sJ = M.f_sJ[face][(size_t)e * NP + q];
@@ -431,14 +433,14 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           double ug[4];
           reflect2(ui, nxo, nyo, ug);
           if (fluidB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !M.curved);
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !curved);
           else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !M.curved);
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         } else {
           double nnx, nny, sJ;
-          if (M.curved) {
+          if (curved) {
             nnx = M.f_nx[fE][(size_t)eA * NP + q];
             nny = M.f_ny[fE][(size_t)eA * NP + q];
             sJ = M.f_sJ[fE][(size_t)eA * NP + q];
@@ -447,7 +449,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
             nny = vert ? 0.0 : 1.0;
             sJ = vert ? sJy[sA] : sJx[sA];
           }
-          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh, !M.curved);
+          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh, !curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
@@ -462,7 +464,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         const double* ui = haveB ? uB : uA;
         if (!(fl & kSlotSolid)) {
           double nxo, nyo, sJ;
-          if (M.curved) {
+          if (curved) {
             nxo = M.f_nx[face][(size_t)e * NP + q];
             nyo = M.f_ny[face][(size_t)e * NP + q];
             sJ = M.f_sJ[face][(size_t)e * NP + q];
@@ -485,9 +487,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           double ug[4];
           exterior<4>(bc, ui, nxo, nyo, X, tstage, ug);
           if (haveB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !M.curved);
+            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !curved);
           else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !M.curved);
+            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !curved);
 #pragma unroll
           for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
         }
@@ -548,7 +550,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double ghW = kBR0 ? fw[4] : 0.0;
       const double ghE = kBR0 ? fw[FS + 4] : 0.0;
       const double rjx = sRjx[s];
-      const double rJa = M.curved ? 0.0 : rjx * sRjy[s];
+      const double rJa = curved ? 0.0 : rjx * sRjy[s];
       const double ev = kAV ? (sEps[s] * rjx) * rjx : 0.0;
       const size_t mrow = (size_t)sEl[s] * NP2 + NP * j;
 #pragma unroll
@@ -556,7 +558,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         double acc = ops.gL[i] * fhW + ops.gR[i] * fhE;
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[i][k] * Fl[k];
-        const double rJ = M.curved ? M.m_rJ[mrow + i] : rJa;
+        const double rJ = curved ? M.m_rJ[mrow + i] : rJa;
         double r = -acc * rJ;
         if (kBR0) {
           double av = 0.0;
@@ -603,7 +605,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double ghS = kBR0 ? fs[4] : 0.0;
       const double ghN = kBR0 ? fs[TX * FS + 4] : 0.0;
       const double rjy = sRjy[s];
-      const double rJa = M.curved ? 0.0 : sRjx[s] * rjy;
+      const double rJa = curved ? 0.0 : sRjx[s] * rjy;
       const double ev = kAV ? (sEps[s] * rjy) * rjy : 0.0;
       const size_t mbase = (size_t)sEl[s] * NP2 + i;
 #pragma unroll
@@ -611,7 +613,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         double acc = ops.gL[j] * fhS + ops.gR[j] * fhN;
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Gl[k];
-        const double rJ = M.curved ? M.m_rJ[mbase + NP * j] : rJa;
+        const double rJ = curved ? M.m_rJ[mbase + NP * j] : rJa;
         double r = -acc * rJ;
         if (kBR0) {
           double av = 0.0;
@@ -799,7 +801,8 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 
 // One tile of one stage (single buffer).  tx0, ty0: first element of the
 // tile.  Used by stage2d_kernel and by the batched kernels.
-template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S, int NTHR = kStageThreads>
+template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S, int NTHR = kStageThreads,
+          int CURV = -1>
 __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
                                              const StageBufs& B, const int tx0, const int ty0) {
   using S = Smem2D<NP, TX, TY, U0S, MINB, NTHR>;
@@ -810,15 +813,15 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
   tile_slots<S>(M, tb, tx0, ty0, ctl.prime);
   __syncthreads();
   tile_issue<NP, AV, S>(M, B, tb, ctl);
-  tile_compute<NP, FLUX, AV, S, 0>(ops, M, P, B, tb, smem, ctl);
+  tile_compute<NP, FLUX, AV, S, 0, CURV>(ops, M, P, B, tb, smem, ctl);
 }
 
 // Single solve, one tile per CTA: the grid covers the mesh with tiles.
 template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
-          bool U0S = true, int NTHR = kStageThreads>
+          bool U0S = true, int NTHR = kStageThreads, int CURV = -1>
 __global__ void __launch_bounds__(NTHR, MINB)
     stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
-  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
+  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR, CURV>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
 }
 
 }  // namespace frg
