@@ -56,12 +56,13 @@ FRG_V(2, 1, 8, 8, 2, true)
 FRG_V(2, 2, 8, 4, 3, false)
 template <>
 struct Variants2D<3> {
-  static constexpr int n = 3, batch = 1;
+  static constexpr int n = 4, batch = 2;
   template <int V> struct V_;
 };
-FRG_V(3, 0, 4, 4, 4, false)
-FRG_V(3, 1, 8, 6, 2, true)
-FRG_V(3, 2, 8, 3, 3, false)
+FRG_VT(3, 0, 8, 8, 2, false, 512)
+FRG_V(3, 1, 4, 4, 4, false)
+FRG_V(3, 2, 8, 6, 2, true)
+FRG_V(3, 3, 8, 3, 3, false)
 template <>
 struct Variants2D<4> {
   static constexpr int n = 5, batch = 1;
