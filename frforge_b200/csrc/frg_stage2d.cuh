@@ -408,6 +408,11 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       }
       double fh[4] = {0.0, 0.0, 0.0, 0.0};
       const int fE = vert ? 1 : 3, fW = vert ? 0 : 2;  // face slots E/N and W/S
+      // The two states and the normal of the numerical flux: the interior
+      // pair, or an element's trace and its ghost state (wall or domain
+      // boundary).  One flux evaluation serves every case.
+      double fL[4], fR[4], fnx = 0.0, fny = 0.0, fsJ = 0.0;
+      bool doflux = false;
       if (eA >= 0 && eB >= 0) {
         const bool solA = flA & kSlotSolid, solB = flB & kSlotSolid;
         const bool wrapf = (flA | flB) & kSlotWrap;
@@ -429,29 +434,35 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
             nyo = vert ? 0.0 : (fluidB ? -1.0 : 1.0);
             sJ = vert ? sJy[fluidB ? sB : sA] : sJx[fluidB ? sB : sA];
           }
-          const double* ui = fluidB ? uB : uA;
-          double ug[4];
+          double ui[4], ug[4];
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) ui[c] = fluidB ? uB[c] : uA[c];
           reflect2(ui, nxo, nyo, ug);
-          if (fluidB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !curved);
-          else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !curved);
 #pragma unroll
-          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
-        } else {
-          double nnx, nny, sJ;
-          if (curved) {
-            nnx = M.f_nx[fE][(size_t)eA * NP + q];
-            nny = M.f_ny[fE][(size_t)eA * NP + q];
-            sJ = M.f_sJ[fE][(size_t)eA * NP + q];
-          } else {
-            nnx = vert ? 1.0 : 0.0;
-            nny = vert ? 0.0 : 1.0;
-            sJ = vert ? sJy[sA] : sJx[sA];
+          for (int c = 0; c < NEQ; ++c) {
+            fL[c] = fluidB ? ug[c] : ui[c];
+            fR[c] = fluidB ? ui[c] : ug[c];
           }
-          iflux2<FLUX>(P.gamma, P.g1, uA, uB, nnx, nny, fh, !curved);
+          fnx = fluidB ? -nxo : nxo;
+          fny = fluidB ? -nyo : nyo;
+          fsJ = sJ;
+          doflux = true;
+        } else {
+          if (curved) {
+            fnx = M.f_nx[fE][(size_t)eA * NP + q];
+            fny = M.f_ny[fE][(size_t)eA * NP + q];
+            fsJ = M.f_sJ[fE][(size_t)eA * NP + q];
+          } else {
+            fnx = vert ? 1.0 : 0.0;
+            fny = vert ? 0.0 : 1.0;
+            fsJ = vert ? sJy[sA] : sJx[sA];
+          }
 #pragma unroll
-          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
+          for (int c = 0; c < NEQ; ++c) {
+            fL[c] = uA[c];
+            fR[c] = uB[c];
+          }
+          doflux = true;
         }
       } else {
         // domain boundary: A missing (left/bottom) or B missing (right/top)
@@ -461,7 +472,6 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         const int fl = haveB ? flB : flA;
         const int face = haveB ? fW : fE;
         const BCDev& bc = M.bc[vert ? (haveB ? 0 : 1) : (haveB ? 2 : 3)];
-        const double* ui = haveB ? uB : uA;
         if (!(fl & kSlotSolid)) {
           double nxo, nyo, sJ;
           if (curved) {
@@ -484,15 +494,25 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
             Y = M.yc[gy] + M.Jy[gy] * (haveB ? -1.0 : 1.0);
           }
           if (M.wavy) X = X + M.amp * sin(6.283185307179586 * Y) * sin(3.141592653589793 * X);
-          double ug[4];
-          exterior<4>(bc, ui, nxo, nyo, X, tstage, ug);
-          if (haveB)
-            iflux2<FLUX>(P.gamma, P.g1, ug, ui, -nxo, -nyo, fh, !curved);
-          else
-            iflux2<FLUX>(P.gamma, P.g1, ui, ug, nxo, nyo, fh, !curved);
+          double ui[4], ug[4];
 #pragma unroll
-          for (int c = 0; c < NEQ; ++c) fh[c] *= sJ;
+          for (int c = 0; c < NEQ; ++c) ui[c] = haveB ? uB[c] : uA[c];
+          exterior<4>(bc, ui, nxo, nyo, X, tstage, ug);
+#pragma unroll
+          for (int c = 0; c < NEQ; ++c) {
+            fL[c] = haveB ? ug[c] : ui[c];
+            fR[c] = haveB ? ui[c] : ug[c];
+          }
+          fnx = haveB ? -nxo : nxo;
+          fny = haveB ? -nyo : nyo;
+          fsJ = sJ;
+          doflux = true;
         }
+      }
+      if (doflux) {
+        iflux2<FLUX>(P.gamma, P.g1, fL, fR, fnx, fny, fh, !curved);
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) fh[c] *= fsJ;
       }
 #pragma unroll
       for (int c = 0; c < NEQ; ++c) out[c] = fh[c];
