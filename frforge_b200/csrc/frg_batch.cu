@@ -156,9 +156,10 @@ struct frg_batch {
 namespace {
 
 constexpr int kMaxReps = 32;  // multirate: most steps per round of one group
-// An instance with at least this many batched tiles (a full wave of resident
-// CTAs on 148 SMs) gains nothing from sharing launches and runs solo.
-constexpr int kSoloTiles = 600;
+// An instance with at least a full wave of resident batched tiles (148 SMs
+// times the batched kernel's CTAs per SM) gains nothing from sharing launches
+// and runs solo.
+constexpr int kSMs = 148;
 
 int bcheck(frg_batch* b, cudaError_t e, const char* what) { return cuda_err(b->ctx, e, what); }
 
@@ -213,10 +214,11 @@ int rebuild(frg_batch* b) {
     const int flux = s->dim == 2 ? s->L2.flux : s->L1.flux;
     const int variant = 0;  // the batched kernels use one fixed tile shape per NP
     int tx = 1, ty = 1;
-    batch_tile_shape(s->dim, s->np, variant, &tx, &ty);
+    const int per_sm = batch_tile_shape(s->dim, s->np, variant, &tx, &ty);
     // the choice depends on the instance alone, so its results do not
     // depend on what else is in the batch
-    const bool solo = s->dim == 2 && (long)((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) >= kSoloTiles;
+    const bool solo =
+        s->dim == 2 && (long)((s->nx + tx - 1) / tx) * ((s->ny + ty - 1) / ty) >= (long)kSMs * per_sm;
     frg_batch::Group* grp = nullptr;
     if (!solo)
       for (auto& g : b->groups)

@@ -74,8 +74,8 @@ FRG_DEV void copy_to_smem(T* dst, const T* src) {
 // The mesh, physics and stage descriptors of the CTA's instance live in
 // static shared memory (at most kBatchStaticSmem bytes), read on demand by the
 // tile function instead of occupying registers.
-template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S>
-__global__ void __launch_bounds__(kStageThreads, MINB)
+template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S, int NTHR = kStageThreads>
+__global__ void __launch_bounds__(NTHR, MINB)
     stage2d_batch_kernel(const OpsT<NP> ops, const BatchInst* __restrict__ insts,
                          const BatchTile* __restrict__ tiles, int stage, int mode) {
   __shared__ __align__(16) Mesh2Dev sM;
@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kStageThreads, MINB)
   copy_to_smem(&sP, &I->P);
   if (threadIdx.x == 0) sB = batch_bufs(*I, stage, mode);
   __syncthreads();
-  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S>(ops, sM, sP, sB, t.x0, t.y0);
+  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR>(ops, sM, sP, sB, t.x0, t.y0);
 }
 
 template <int NP, int FLUX, int AV>

@@ -204,6 +204,8 @@ int launch_batch2d(const HostOps* ops, int flux, int av, int variant, const Batc
                    const BatchTile* tiles, int ntiles, int stage, int mode, void* stream);
 int launch_batch1d(const HostOps* ops, int flux, int av, const BatchInst* insts,
                    const BatchTile* tiles, int ntiles, int stage, int mode, void* stream);
+// Tile shape of the batched kernels; returns their CTAs per SM (2D), 1 (1D)
+// or -1 (unsupported NP).
 int batch_tile_shape(int dim, int np, int variant, int* tx, int* ty);
 int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream);
 int stage2d_variants(int np);

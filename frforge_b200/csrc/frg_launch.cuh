@@ -56,7 +56,7 @@ FRG_V(2, 1, 8, 8, 2, true)
 FRG_V(2, 2, 8, 4, 3, false)
 template <>
 struct Variants2D<3> {
-  static constexpr int n = 4, batch = 2;
+  static constexpr int n = 4, batch = 0;
   template <int V> struct V_;
 };
 FRG_VT(3, 0, 8, 8, 2, false, 512)
@@ -65,7 +65,7 @@ FRG_V(3, 2, 8, 6, 2, true)
 FRG_V(3, 3, 8, 3, 3, false)
 template <>
 struct Variants2D<4> {
-  static constexpr int n = 5, batch = 1;
+  static constexpr int n = 5, batch = 0;
   template <int V> struct V_;
 };
 FRG_VT(4, 0, 8, 4, 2, false, 512)
@@ -75,7 +75,7 @@ FRG_V(4, 3, 8, 4, 2, true)
 FRG_V(4, 4, 4, 4, 4, false)
 template <>
 struct Variants2D<5> {
-  static constexpr int n = 3, batch = 1;
+  static constexpr int n = 3, batch = 0;
   template <int V> struct V_;
 };
 FRG_VT(5, 0, 8, 3, 2, false, 512)
@@ -83,7 +83,7 @@ FRG_V(5, 1, 4, 3, 3, false)
 FRG_V(5, 2, 4, 4, 2, true)
 template <>
 struct Variants2D<6> {
-  static constexpr int n = 3, batch = 1;
+  static constexpr int n = 3, batch = 0;
   template <int V> struct V_;
 };
 FRG_VT(6, 0, 6, 3, 2, false, 512)
@@ -188,16 +188,15 @@ template <int NP, int FLUX, int AV, int V>
 int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles, int ntiles, int stage,
                 int mode, cudaStream_t st) {
   using VV = typename Variants2D<NP>::template V_<V>;
-  static_assert(VV::NT == kStageThreads, "the batched kernels run kStageThreads per CTA");
-  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB>;
-  auto kern = stage2d_batch_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S>;
+  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB, VV::NT>;
+  auto kern = stage2d_batch_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
     if (e != cudaSuccess) return (int)e;
     configured = true;
   }
-  if (ntiles > 0) kern<<<ntiles, kStageThreads, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
+  if (ntiles > 0) kern<<<ntiles, VV::NT, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
   return (int)cudaGetLastError();
 }
 
@@ -261,12 +260,12 @@ int tile_shape_np(int dim, int /*variant*/, int* tx, int* ty) {
   if (dim == 1) {
     *tx = Tile1D<NP>::TX;
     *ty = 1;
-    return 0;
+    return 1;
   }
   using VB = typename Variants2D<NP>::template V_<Variants2D<NP>::batch>;
   *tx = VB::TX;
   *ty = VB::TY;
-  return 0;
+  return VB::MINB;
 }
 
 template <int NP>

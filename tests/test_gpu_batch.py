@@ -147,8 +147,9 @@ def test_batch_mix_matches_solo_bitwise_and_single_path():
 
 
 def test_large_instances_run_solo_bitwise_equal_to_single_path():
-    # 200^2 P=3 RK3 (1,250 batched tiles) and 200^2 P=2 RK2 (850) run solo;
-    # the 12^2 instance is batched beside them
+    # 200^2 P=3 RK3 (1,250 batched 8x4 tiles) and 200^2 P=2 RK2 (625 8x8
+    # tiles) fill a wave of 296 resident tiles and run solo; the 12^2
+    # instance is batched beside them
     cases = [
         (dict(dim=2, p=3, nx=200, ny=200, flux="hllc", method="persson", bcs=("transmissive",) * 4), "quad",
          dict(t_final=1.0, cfl=0.1, max_steps=6)),
