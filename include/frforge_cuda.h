@@ -207,8 +207,8 @@ int frg_step(frg_solve* s, double dt, int* step_status);
 int frg_advance(frg_solve* s, double t_final, double cfl, double fixed_dt,
                 int64_t max_steps, frg_result* out);
 
-/* Stage-kernel tile variants (elements per CTA, CTAs per SM, u0 staging),
-   no reference counterpart.  frg_autotune times every variant on the
+/* Stage-kernel tile variants (elements per CTA, threads per CTA, CTAs per
+   SM, u0 staging), no reference counterpart.  frg_autotune times every variant on the
    solve's current state (scratch buffers only; the state is untouched) with
    `reps` launches each, selects the fastest and returns it in *best; ms (may
    be NULL) receives the mean launch time of each variant. */
