@@ -318,6 +318,75 @@ def run_ours(args):
     return 0
 
 
+def run_c1(args):
+    """The 1D case: 256 elements, P=3, Rusanov, Persson BR0, two-state
+    Riemann IC, 2000 SSP-RK3 steps at CFL 0.1 (3,072 DOF).  It is launch- and
+    latency-bound, not bandwidth-bound, so it reports steps/s and DOF-stage/s
+    without a roofline.  One GPU (rank 0); other ranks exit."""
+    import torch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import frforge_b200 as F
+    from frforge_b200.workloads import C1
+
+    ctx = F.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=torch.device("cuda", 0))
+    st, method = C1.build(F)
+    solve = F.GpuSolve(st, F.Euler1D(1.4), method, ctx=ctx)
+    ndof = solve.ndof
+    u_host = torch.empty(ndof, dtype=torch.float64, pin_memory=True)
+    u_host.numpy()[:] = st.u.ravel(order="F")
+    u_out = torch.empty(ndof, dtype=torch.float64, pin_memory=True)
+    steps = C1.steps
+    for _ in range(max(3, args.warmup)):  # untimed: graph capture, caches
+        solve.upload(st.u, 0.0)
+        solve.advance(1e9, cfl=C1.cfl, max_steps=steps)
+    times, e2e_times = [], []
+    with ClockSampler(0) as clk:
+        for _ in range(max(1, args.batch_reps)):
+            solve.upload(st.u, 0.0)
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            r = solve.advance(1e9, cfl=C1.cfl, max_steps=steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            if r["status"] != "max_steps" or r["n_steps"] != steps:
+                raise RuntimeError(f"C1 run ended early: {r}")
+            times.append(ev0.elapsed_time(ev1))
+            # end to end through the C ABI: upload, the 2000 steps, download
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            solve.upload_ptr(u_host.data_ptr(), 0.0)
+            solve.advance(1e9, cfl=C1.cfl, max_steps=steps)
+            solve.download_ptr(u_out.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    ms_e2e = float(np.median(e2e_times))
+    line = {
+        "metric": "C1 1D solve: SSP-RK3 steps/s and DOF-stage/s (launch-bound, no roofline)",
+        "value": steps / (ms * 1e-3), "unit": "steps/s", "n_gpus": 1, "steps": steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded two-state Riemann IC)",
+        "config": {"workload": "1D Euler, 256 elements on [0,1], GL P=3, Rusanov, SSP-RK3, Persson AV (BR0, "
+                               "c_av=0.1), transmissive, CFL 0.1, 2000 steps, seeded two-state Riemann IC",
+                   "dof": ndof, "repeats": len(times)},
+        "dof_stage_per_s": 3 * ndof * steps / (ms * 1e-3),
+        "e2e": {"value": steps / (ms_e2e * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": ndof * 8 / steps,
+                "d2h_bytes_per_step": ndof * 8 / steps},
+        "clocks": clk.summary(),
+        "gpu_launches": steps * 5,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_batched(args):
     """64 independent mixed solves (frforge_b200.workloads.c4_instances), each
     200 SSP-RK3 steps: solves/s of the batched engine (frg_batch_*) against
@@ -576,7 +645,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c3", choices=["c3", "batched", "served"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c1", "batched", "served"])
     ap.add_argument("--served-requests", type=int, default=32)
     ap.add_argument("--ncu-target", action="store_true")
     ap.add_argument("--n", type=int, default=512)
@@ -591,6 +660,8 @@ def main():
         return run_ncu_target(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "c1":
+        return run_c1(args)
     if args.workload == "served":
         return run_served(args)
     return run_ours(args)

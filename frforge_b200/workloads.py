@@ -114,6 +114,42 @@ class Workload2D:
         return four_quadrant_ic(X, Y, four_quadrant_states(self.seed, self.jump_scale))
 
 
+@dataclass
+class Workload1D:
+    name: str
+    nel: int
+    p: int
+    flux: str
+    method: str
+    c_av: float
+    cfl: float
+    steps: int
+    seed: int = DEFAULT_SEED
+
+    @property
+    def ndof(self) -> int:
+        return self.nel * (self.p + 1) * 3
+
+    def build(self, F):
+        """(state, method) for the frforge_b200 module F, IC filled in."""
+        mesh = F.Mesh1D(0.0, 1.0, self.nel, F.TransmissiveBC(), F.TransmissiveBC())
+        ops = F.build_operators(self.p)
+        st = F.allocate_state(mesh, ops, 3, scheme=F.SchemeConfig("gl", self.flux, "ssp_rk3"))
+        st.u[...] = self.initial_state(mesh.physical_coords(ops))
+        m = F.PerssonAVMethod(c_av=self.c_av) if self.method == "persson_av" else F.NullCapturing()
+        return st, m
+
+    def initial_state(self, x, gamma: float = 1.4) -> np.ndarray:
+        """Two states split at x = 0.5 (left for x < 0.5, as sod_ic)."""
+        (rL, uL, pL), (rR, uR, pR) = two_state_1d(self.seed)
+        left = x < 0.5
+        r = np.where(left, rL, rR)
+        u = np.where(left, uL, uR)
+        p = np.where(left, pL, pR)
+        return np.stack([r, r * u, p / (gamma - 1.0) + 0.5 * r * u * u], axis=-1)
+
+
+C1 = Workload1D("c1", 256, 3, "rusanov", "persson_av", 0.1, 0.1, 2000)
 C2 = Workload2D("c2", 128, 4, "rusanov", "persson_av", 0.1, True, 0.1, 500)
 C3 = Workload2D("c3", 512, 3, "hllc", "persson_av", 0.1, False, 0.1, 1000)
 WORKLOADS = {"c2": C2, "c3": C3}

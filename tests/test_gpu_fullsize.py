@@ -15,7 +15,7 @@ import pytest
 
 import frforge_b200 as F
 import oracle as O
-from frforge_b200.workloads import C2, C3
+from frforge_b200.workloads import C1, C2, C3
 
 pytestmark = pytest.mark.gpu
 
@@ -64,3 +64,20 @@ def test_128sq_p4_periodic_100_steps_and_mass():
     for c in range(4):
         assert abs(d["mass"][c] - mass0[c]) <= 1e-12 * max(abs(mass0[c]), 1.0), c
     assert d["positivity_ok"] and d["nonfinite"] == 0
+
+
+def test_c1_1d_full_length():
+    # the 1D case at its full length: 256 elements, P=3, 2000 SSP-RK3 steps
+    st, m = C1.build(F)
+    O.set_threads(os.cpu_count() or 1)
+    orc = O.OracleSolver.one_d(p=C1.p, nel=C1.nel, flux=C1.flux, method="persson", c_av=C1.c_av)
+    orc.set_state(st.u)
+    r_ref = orc.integrate(1e9, cfl=C1.cfl, max_steps=C1.steps)
+    s = F.GpuSolve(st, F.Euler1D(1.4), m)
+    s.upload(st.u, 0.0)
+    r = s.advance(1e9, cfl=C1.cfl, max_steps=C1.steps)
+    u, t = s.download()
+    assert r["status"] == r_ref["status"] == "max_steps" and r["n_steps"] == r_ref["n_steps"] == C1.steps
+    assert t == pytest.approx(orc.t, rel=1e-12)
+    # shocked state: relative L1 to 1e-8
+    assert _rel_l1(u, orc.u) <= 1e-8
