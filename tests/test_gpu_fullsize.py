@@ -8,6 +8,7 @@
 
 The oracle runs with all host threads; each case takes seconds on the host.
 """
+import math
 import os
 
 import numpy as np
@@ -81,3 +82,34 @@ def test_c1_1d_full_length():
     assert t == pytest.approx(orc.t, rel=1e-12)
     # shocked state: relative L1 to 1e-8
     assert _rel_l1(u, orc.u) <= 1e-8
+
+
+def test_c2_smooth_order_p4():
+    # run_euler2d_smooth_order (src/verification/Cases2D_Smooth.jl:94-150) at
+    # P=4: NullCapturing, t_final 0.25, fixed dt from the finest mesh
+    # (dt = cfl/(p+1) h/((2p+1) lambda), lambda = 1 + sqrt(gamma), cfl 0.06),
+    # the smooth wave evaluated and measured on the device; observed orders
+    # must reach formal - 0.3 (order_pass, src/verification/Metrics.jl:34-45).
+    # At P=4 the density L2 error meets the FP64 round-off floor of the time
+    # loop (about 1.3e-12 after 21,000 steps, measured at n = 128 and 256), so
+    # the meshes are n = 16..64, whose errors lie above it (n = 8 is still
+    # pre-asymptotic: order 4.69 from 8 to 16).  Measured orders 4.91, 4.97.
+    p, n_list, t_final, cfl, gamma = 4, [16, 32, 64], 0.25, 0.06, 1.4
+    lam = 1.0 + math.sqrt(gamma)
+    dt = (cfl / (p + 1)) * (1.0 / max(n_list)) / ((2 * p + 1) * lam)
+    errs = []
+    for n in n_list:
+        bc = F.PeriodicBC
+        mesh = F.Mesh2D(0.0, 1.0, 0.0, 1.0, n, n, bc(), bc(), bc(), bc())
+        st = F.allocate_state(mesh, F.build_operators(p), 4)
+        s = F.GpuSolve(st, F.Euler2D(gamma), F.NullCapturing())
+        s.set_initial_condition("smooth_2d")
+        r = s.advance(t_final, dt=dt)
+        assert r["status"] == "ok", n
+        d = s.diagnostics(exact="smooth_2d", t_exact=t_final)
+        assert d["t"] == pytest.approx(t_final, abs=1e-14) and d["nonfinite"] == 0
+        errs.append(d["l2_error"])
+        s.close()
+    assert errs[-1] > 1e-11  # above the round-off floor
+    orders = [math.log(errs[k] / errs[k + 1]) / math.log(2.0) for k in range(len(errs) - 1)]
+    assert all(q >= (p + 1) - 0.3 for q in orders), (errs, orders)
