@@ -33,7 +33,7 @@ OpsT<NP> make_ops(const HostOps& h) {
 }
 
 // Tile variants per NP: (TX, TY, CTAs per SM, u0 staged in shared memory,
-// and for FRG_VT the threads per CTA, else 256).
+// and for FRG_VT the threads per CTA, a multiple of 32, else 256).
 // Variant 0 is the default, the fastest measured on a B200 for large meshes
 // (P<=3: 512^2, P=4/5: 384^2); the autotuner times all of them on the solve.
 // The batched kernels use variant `batch`.
@@ -48,12 +48,13 @@ struct Variants2D;
 #define FRG_V(NPv, idx, tx, ty, minb, u0s) FRG_VT(NPv, idx, tx, ty, minb, u0s, kStageThreads)
 template <>
 struct Variants2D<2> {
-  static constexpr int n = 3, batch = 2;
+  static constexpr int n = 4, batch = 3;
   template <int V> struct V_;
 };
-FRG_VT(2, 0, 16, 8, 2, false, 512)
-FRG_V(2, 1, 8, 8, 2, true)
-FRG_V(2, 2, 8, 4, 3, false)
+FRG_VT(2, 0, 16, 6, 2, false, 384)
+FRG_VT(2, 1, 16, 8, 2, false, 512)
+FRG_V(2, 2, 8, 8, 2, true)
+FRG_V(2, 3, 8, 4, 3, false)
 template <>
 struct Variants2D<3> {
   static constexpr int n = 4, batch = 0;
