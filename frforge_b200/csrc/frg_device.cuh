@@ -33,12 +33,30 @@ FRG_DEV double jmin(double a, double b) {
   return (a != a) ? a : ((b != b) ? b : r);
 }
 
+// 1/x for the flux kernels: the hardware estimate of PTX rcp.approx.ftz.f64
+// refined by two Newton-Raphson steps y <- y + y (1 - x y), each of which
+// about doubles the number of correct bits (Markstein, IBM J. Res. Dev. 34
+// (1990) 111-119); the result is within 1 ulp of the correctly rounded 1/x
+// for finite x with 2^-1022 <= |x| < 2^1022 (checked against CUDA's division
+// by tests/test_gpu_reciprocal.py).  It replaces the divisions of the flux
+// and wave-speed formulas, whose operands are floored densities or guarded
+// denominators; x = 0 gives NaN where the exact division gives an infinity,
+// and either is caught as non-finite by the stage kernels.
+FRG_DEV double frcp(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
 // ---------------------------------------------------------------- 2D Euler
 
 // Physical fluxes F(U), G(U): physical_flux_x!/y!, Euler2D.jl:54-79.
 FRG_DEV void flux_xy(double g1, const double U[4], double F[4], double G[4]) {
   const double r = jfloor(U[0], kEps);
-  const double ri = 1.0 / r;
+  const double ri = frcp(r);
   const double u = U[1] * ri, v = U[2] * ri;
   const double p = g1 * (U[3] - 0.5 * r * (u * u + v * v));
   F[0] = U[1];
@@ -54,7 +72,7 @@ FRG_DEV void flux_xy(double g1, const double U[4], double F[4], double G[4]) {
 // max(|u|+c, |v|+c) at one state: max_wave_speed, Euler2D.jl:92-105.
 FRG_DEV double wave_speed2(double gamma, double g1, const double U[4]) {
   const double r = jfloor(U[0], kEps);
-  const double ri = 1.0 / r;
+  const double ri = frcp(r);
   const double u = U[1] * ri, v = U[2] * ri;
   const double p = jfloor(g1 * (U[3] - 0.5 * r * (u * u + v * v)), kEps);
   const double c = sqrt(gamma * p * ri);
@@ -64,10 +82,10 @@ FRG_DEV double wave_speed2(double gamma, double g1, const double U[4]) {
 // Rusanov normal flux, numerical_flux_n!, Euler2D.jl:114-150.
 FRG_DEV void rusanov2(double gamma, double g1, const double uL[4], const double uR[4],
                       double nx, double ny, double out[4]) {
-  const double rL = jfloor(uL[0], kEps), riL = 1.0 / rL;
+  const double rL = jfloor(uL[0], kEps), riL = frcp(rL);
   const double uLv = uL[1] * riL, vLv = uL[2] * riL;
   const double pL = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
-  const double rR = jfloor(uR[0], kEps), riR = 1.0 / rR;
+  const double rR = jfloor(uR[0], kEps), riR = frcp(rR);
   const double uRv = uR[1] * riR, vRv = uR[2] * riR;
   const double pR = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
   const double unL = uLv * nx + vLv * ny, unR = uRv * nx + vRv * ny;
@@ -104,8 +122,8 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
     nx = nxi * rn;
     ny = nyi * rn;
   }
-  const double rL = jfloor(uL[0], kEps), riL = 1.0 / rL;
-  const double rR = jfloor(uR[0], kEps), riR = 1.0 / rR;
+  const double rL = jfloor(uL[0], kEps), riL = frcp(rL);
+  const double rR = jfloor(uR[0], kEps), riR = frcp(rR);
   const double uLv = uL[1] * riL, vLv = uL[2] * riL;
   const double uRv = uR[1] * riR, vRv = uR[2] * riR;
   const double pLu = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
@@ -117,7 +135,7 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
   const double SR = jmax(unL + cL, unR + cR);
   const double num = pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR);
   const double den = rL * (SL - unL) - rR * (SR - unR);
-  const double SM = fabs(den) < kEps ? 0.5 * (unL + unR) : num / den;
+  const double SM = fabs(den) < kEps ? 0.5 * (unL + unR) : num * frcp(den);
   // F.n with the unfloored pressure of physical_flux_x!/y!
   if (0.0 <= SL) {
     out[0] = uL[1] * nx + uL[2] * ny;
@@ -147,7 +165,7 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
   const double vstar = (v - un * ny) + SM * ny;
   const double Sun = S - un;
   // the two remaining divisions are independent reciprocals
-  const double rB = 1.0 / (S - SM), rA = 1.0 / (r * Sun);
+  const double rB = frcp(S - SM), rA = frcp(r * Sun);
   const double factor = r * Sun * rB;
   const double estar = U[3] * ri + (SM - un) * (SM + p * rA);
   out[0] = F0 + S * (factor - U[0]);
@@ -316,7 +334,7 @@ FRG_DEV double persson_sigma(double e_high, double e_tot, double s0, double kapp
 FRG_DEV double br0_tau(double em, double ep, double hm, double hp, int p) {
   const double eb = 0.5 * (em + ep);
   const double hb = 0.5 * (hm + hp);
-  return 2.0 * eb * (double)(p + 1) / jmax(hb, kEps);
+  return 2.0 * eb * (double)(p + 1) * frcp(jmax(hb, kEps));
 }
 
 // atomic max of a non-negative double via its bit pattern (NaN sorts high)
