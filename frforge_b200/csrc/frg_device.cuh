@@ -51,6 +51,29 @@ FRG_DEV double frcp(double x) {
   return fma(y, e, y);
 }
 
+// sqrt(x) for the sound speeds of the flux kernels: Goldschmidt's coupled
+// iteration for g -> sqrt(x) and h -> 1/(2 sqrt(x)) (r = 1/2 - g h;
+// g += g r; h += h r; Goldschmidt 1964, as in Markstein, "IA-64 and
+// Elementary Functions", 2000), started from the PTX rsqrt.approx.ftz.f64
+// estimate, two iterations and one residual correction g + (x - g^2) h.
+// Within 1 ulp of CUDA's correctly rounded sqrt for positive normal x
+// (tests/test_gpu_reciprocal.py); the operands are gamma p / rho with p and
+// rho floored at eps, so always positive.  x = 0 gives NaN.
+FRG_DEV double fsqrt(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double h = 0.5 * y;
+  double g = x * y;
+  double r = fma(-g, h, 0.5);
+  g = fma(g, r, g);
+  h = fma(h, r, h);
+  r = fma(-g, h, 0.5);
+  g = fma(g, r, g);
+  h = fma(h, r, h);
+  const double d = fma(-g, g, x);
+  return fma(d, h, g);
+}
+
 // ---------------------------------------------------------------- 2D Euler
 
 // Physical fluxes F(U), G(U): physical_flux_x!/y!, Euler2D.jl:54-79.
@@ -75,7 +98,7 @@ FRG_DEV double wave_speed2(double gamma, double g1, const double U[4]) {
   const double ri = frcp(r);
   const double u = U[1] * ri, v = U[2] * ri;
   const double p = jfloor(g1 * (U[3] - 0.5 * r * (u * u + v * v)), kEps);
-  const double c = sqrt(gamma * p * ri);
+  const double c = fsqrt(gamma * p * ri);
   return jmax(fabs(u) + c, fabs(v) + c);
 }
 
@@ -97,8 +120,8 @@ FRG_DEV void rusanov2(double gamma, double g1, const double uL[4], const double 
   const double fR1 = (uR[1] * uRv + pR) * nx + (uR[1] * vRv) * ny;
   const double fR2 = (uR[2] * uRv) * nx + (uR[2] * vRv + pR) * ny;
   const double fR3 = (uR[3] + pR) * unR;
-  const double cL = sqrt(gamma * jfloor(pL, kEps) * riL);
-  const double cR = sqrt(gamma * jfloor(pR, kEps) * riR);
+  const double cL = fsqrt(gamma * jfloor(pL, kEps) * riL);
+  const double cR = fsqrt(gamma * jfloor(pR, kEps) * riR);
   const double lam = jmax(fabs(unL) + cL, fabs(unR) + cR);
   const double hl = 0.5 * lam;
   out[0] = 0.5 * (fL0 + fR0) - hl * (uR[0] - uL[0]);
@@ -130,7 +153,7 @@ FRG_DEV void hllc2(double gamma, double g1, const double uL[4], const double uR[
   const double pRu = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
   const double pL = jfloor(pLu, kEps), pR = jfloor(pRu, kEps);
   const double unL = uLv * nx + vLv * ny, unR = uRv * nx + vRv * ny;
-  const double cL = sqrt(gamma * pL * riL), cR = sqrt(gamma * pR * riR);
+  const double cL = fsqrt(gamma * pL * riL), cR = fsqrt(gamma * pR * riR);
   const double SL = jmin(unL - cL, unR - cR);
   const double SR = jmax(unL + cL, unR + cR);
   const double num = pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR);

@@ -1,8 +1,9 @@
-"""The reciprocal the stage kernels use in their flux and wave-speed
-formulas (frcp in frforge_b200/csrc/frg_device.cuh: hardware estimate plus
-two Newton-Raphson steps) against CUDA's correctly rounded division on the
-same device: within 1 ulp over the operand range the kernels use, and
-non-finite where the exact quotient is."""
+"""The reciprocal and square root the stage kernels use in their flux and
+wave-speed formulas (frcp and fsqrt in frforge_b200/csrc/frg_device.cuh:
+hardware estimates refined by Newton-Raphson and Goldschmidt iterations)
+against CUDA's correctly rounded division and sqrt on the same device:
+within 1 ulp over the operand ranges the kernels use, and non-finite where
+the exact result is."""
 import ctypes as C
 
 import numpy as np
@@ -13,9 +14,9 @@ from frforge_b200 import _lib as L
 pytestmark = pytest.mark.gpu
 
 
-def _check(x):
+def _check(x, name="frg_internal_reciprocal_check"):
     lib = L.load()
-    fn = lib.frg_internal_reciprocal_check
+    fn = getattr(lib, name)
     fn.restype = C.c_int
     fn.argtypes = [C.POINTER(C.c_double)] * 3 + [C.c_size_t]
     x = np.ascontiguousarray(x, dtype=np.float64)
@@ -53,3 +54,17 @@ def test_reciprocal_non_finite_cases():
     # NaN there, which the stage kernels flag like the exact infinities
     assert np.isnan(y[0]) and np.isinf(q[0])
     assert np.isnan(y[3]) and np.isnan(q[3])
+
+
+def test_sqrt_within_one_ulp():
+    rng = np.random.default_rng(20261204)
+    e = rng.integers(-1000, 1000, size=200000)
+    x = np.ldexp(rng.uniform(1.0, 2.0, size=e.size), e)
+    # sound-speed operands gamma p / rho with floored p and rho
+    x = np.concatenate([x, [1.4 * 2.220446049250313e-16, 1.4, 0.56, 1.4e-16 / 3.0, 4.0, 2.0, 1e-300, 1e300]])
+    y, q = _check(x, "frg_internal_sqrt_check")
+    assert np.all(np.isfinite(y)) and np.all(np.isfinite(q))
+    assert int(_ulps(y, q).max()) <= 1
+    assert np.mean(y == q) > 0.9
+    y, q = _check(np.array([np.nan, np.inf]), "frg_internal_sqrt_check")
+    assert np.isnan(y[0]) and not np.isfinite(y[1])
