@@ -349,8 +349,10 @@ FRG_DEV void exterior1(const BCDev& bc, const double* ui, double nx, double* ug)
 
 // Persson logistic indicator, SharedAV.jl:9-21
 FRG_DEV double persson_sigma(double e_high, double e_tot, double s0, double kappa, double ef) {
-  const double se = log10(e_high / e_tot + ef);
-  return 1.0 / (1.0 + exp(-kappa * (se - s0)));
+  // the quotients by frcp: one warp finishes a tile's elements here, so its
+  // latency is the tile's tail
+  const double se = log10(e_high * frcp(e_tot) + ef);
+  return frcp(1.0 + exp(-kappa * (se - s0)));
 }
 
 // BR0 interior penalty and average, SharedAV.jl:29-42

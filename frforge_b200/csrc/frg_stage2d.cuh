@@ -808,7 +808,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         continue;
       }
       double ev = 0.0;
-      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (sHc[s] / (double)P.pm) * lam;
+      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (sHc[s] * frcp((double)P.pm)) * lam;
       B.eps_out[el] = ev;
     }
     // the warps that hold elements (NOWN <= NT)
