@@ -798,8 +798,17 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         etot += sPart[o * PS + 2 * i + 0];
         ehigh += sPart[o * PS + 2 * i + 1];
       }
+      {
+        // pairwise (depth log2 NP2): the same maximum, a shorter chain
+        double w[NP2];
 #pragma unroll
-      for (int k = 0; k < NP2; ++k) lam = jmax(lam, sWS[o * WS + k]);
+        for (int k = 0; k < NP2; ++k) w[k] = sWS[o * WS + k];
+#pragma unroll
+        for (int h = 1; h < NP2; h *= 2)
+#pragma unroll
+          for (int k = 0; k + h < NP2; k += 2 * h) w[k] = jmax(w[k], w[k + h]);
+        lam = jmax(lam, w[0]);
+      }
       lcta = jmax(lcta, lam);
       lam = jmax(lam, kEps);
       const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
