@@ -343,8 +343,9 @@ def run_c1(args):
         solve.upload(st.u, 0.0)
         solve.advance(1e9, cfl=C1.cfl, max_steps=steps)
     times, e2e_times = [], []
+    repeats = max(1, args.batch_reps)  # --batch-reps: timed repeats of the 2000 steps (median reported)
     with ClockSampler(0) as clk:
-        for _ in range(max(1, args.batch_reps)):
+        for _ in range(repeats):
             solve.upload(st.u, 0.0)
             ev0 = torch.cuda.Event(enable_timing=True)
             ev1 = torch.cuda.Event(enable_timing=True)
