@@ -9,9 +9,10 @@
 //   P1  physical fluxes -> contravariant F~, G~ at every own solution point
 //       (Residual2D.jl:342-352)
 //   P2  every face point of the tile once: u traces of both sides
-//       (face_trace!, Residual2D.jl:9-48), Rusanov/HLLC or the boundary
-//       ghost flux times sJ (Residual2D.jl:173-334), and for BR0 the g traces
-//       and the averaged viscous flux g^ (PerssonAV2D.jl:228-350)
+//       (face_trace!, Residual2D.jl:9-48), for BR0 the g traces and the
+//       averaged viscous flux g^ (PerssonAV2D.jl:228-350), then one
+//       Rusanov/HLLC evaluation on the interior pair or on a trace and its
+//       wall / boundary ghost state, times sJ (Residual2D.jl:173-334)
 //   P3  xi-direction divergence + g_DG lift (Residual2D.jl:354-374) and the
 //       BR0 / D(Du) x-terms (PerssonAV2D.jl:135-194, :352-375)
 //   P4  eta-direction terms (Residual2D.jl:376-396, PerssonAV2D.jl:376-395),
@@ -21,15 +22,18 @@
 //   P6  sensor of the NEW state (sense!, PerssonAV2D.jl:20-59), element
 //       viscosity eps for the next stage (element_viscosities_2d,
 //       PerssonAV2D.jl:89-109) and the CFL wave speed (compute_dt,
-//       SSP_RK3.jl:126-133) as one atomic max per tile.
+//       SSP_RK3.jl:126-133) as one atomic max per tile of its elements'
+//       maxima.
 // Halo values come from the neighbouring tiles' own loads, so they are
 // L2 hits; DRAM traffic per stage is the algorithmic u_s + u0 + u_out.
 //
 // The single-solve kernel and the batched kernels run one tile per CTA
-// through the same phases (tile_slots / tile_issue / tile_compute).  A
-// persistent variant that copied each CTA's next tile into a second buffer
-// while computing the current one measured slower on a B200: with four
-// resident CTAs per SM the other CTAs already cover the load latency.
+// through the same phases (tile_slots / tile_issue / tile_compute); tile
+// variants differ in tile shape, threads per CTA (256, 384 or 512) and CTAs
+// per SM, and the single-solve kernel has affine and curved instantiations.
+// A persistent variant that copied each CTA's next tile into a second buffer
+// while computing the current one measured slower on a B200: the other
+// resident CTAs already cover the load latency.
 //
 // Shared-memory blocks use odd strides (in doubles) between elements and
 // lanes walk over elements first, so a warp's 8-byte accesses spread over
