@@ -17,7 +17,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _lib as L
-from .gpu import Context, default_context, diagnostics_of, make_desc
+from .gpu import Context, default_context, diagnostics_of, make_desc, set_solve_hooks
 from .methods import AbstractCapturingMethod
 
 
@@ -28,13 +28,6 @@ def solve_bytes(state, eq, method: Optional[AbstractCapturingMethod] = None,
     n = C.c_size_t()
     L.check(L.load().frg_solve_bytes(C.byref(d), C.byref(n)), None, "frg_solve_bytes")
     return int(n.value)
-
-
-def _refuse_hooks(method) -> None:
-    """Batched instances run no device hooks (frg_batch_start refuses them)."""
-    if method is not None and method.gpu_spec().get("hooks"):
-        raise L.UnsupportedHookError(L.FRG_ERR_UNSUPPORTED_HOOK,
-                                     f"{type(method).__name__}: batched instances run no post-step hook")
 
 
 class Batch:
@@ -79,12 +72,17 @@ class Batch:
             caller_ops=None) -> int:
         """Create an instance for ``state`` (its u and t are uploaded); returns
         its slot.  Raises FRGError (FRG_ERR_OOM) when the batch is full or its
-        HBM budget would be exceeded."""
-        _refuse_hooks(method)
+        HBM budget would be exceeded.  The device hooks the method selects
+        (post_step) run on the instance after each of its completed steps."""
         d, _keep = make_desc(state, eq, method, time, caller_ops)
         slot = C.c_int()
         self._chk(L.load().frg_batch_add(self.handle, C.byref(d), C.byref(slot)), "frg_batch_add")
         i = slot.value
+        try:
+            set_solve_hooks(self._solve(i), self.ctx, method)
+        except Exception:
+            self.remove(i)
+            raise
         self._shape[i] = state.u.shape
         self._ndof[i] = int(state.u.size)
         self.upload(i, state.u, state.t)

@@ -153,8 +153,9 @@ int launch(frg_solve* s, const StageBufs& b) {
 
 bool needs_eps(const frg_solve* s) { return s->method == FRG_METHOD_PERSSON; }
 
-// Element viscosity and wave speed of the state in buffer `buf` (prime mode).
-int prime(frg_solve* s, int buf, bool want_lambda) {
+// Element viscosity and wave speed of the state in buffer `buf` (prime mode),
+// on the solve's stream or on `st`.
+int prime_on(frg_solve* s, int buf, bool want_lambda, cudaStream_t st) {
   if (!needs_eps(s) && !want_lambda) return FRG_OK;
   StageBufs b{};
   b.us = s->U[buf];
@@ -162,8 +163,10 @@ int prime(frg_solve* s, int buf, bool want_lambda) {
   b.mode = kModePrime;
   b.want_lambda = want_lambda;
   b.sc = s->sc;
-  return launch(s, b);
+  const int e = s->dim == 2 ? launch_stage2d(s->L2, b, st) : launch_stage1d(s->L1, b, st);
+  return e ? cuda_err(s->ctx, (cudaError_t)e, "stage kernel launch") : FRG_OK;
 }
+int prime(frg_solve* s, int buf, bool want_lambda) { return prime_on(s, buf, want_lambda, s->ctx->stream); }
 
 // Stage buffers of SSP-RK stage `stage` of a solve (buffer rotation U0 ->
 // U1 -> U2 -> U0, SSP_RK3.jl:135-164 / SSP_RK2.jl:42-48).

@@ -126,6 +126,8 @@ struct frg_batch {
   int* h_nrun = nullptr;  // pinned
   struct Group {
     int dim, np, flux, av, variant;
+    int hook = 0;     // post-step hook id shared by the members (kHookNone: none)
+    int tx = 1, ty = 1;  // tile shape of the batched kernels
     // solo: one instance large enough to fill the device by itself, stepped
     // with the single-solve stage kernels (its own tuned tile shape)
     bool solo = false;
@@ -140,6 +142,7 @@ struct frg_batch {
     const int* d_members() const { return (const int*)((const char*)d_buf + sizeof(BatchTile) * tiles.size()); }
   };
   std::vector<Group> groups;
+  std::vector<BatchInst> h_insts;  // the instance table as last uploaded
   // groups advance as parallel branches: an instance's stages depend only on
   // its own previous stage
   static constexpr int kAux = 16;
@@ -177,6 +180,9 @@ BatchInst inst_of(frg_solve* s) {
   I.sc = s->sc;
   I.rk2 = s->time_scheme == FRG_TIME_SSP_RK2;
   I.dim = s->dim;
+  I.hook = s->post_step_id;
+  I.hook_params[0] = s->post_step_params[0];
+  I.hook_params[1] = s->post_step_params[1];
   return I;
 }
 
@@ -184,7 +190,7 @@ bool same_tables(const HostOps& a, const HostOps& b) {
   if (a.np != b.np) return false;
   const int n = a.np;
   for (int i = 0; i < n; ++i) {
-    if (a.xi[i] != b.xi[i] || a.lL[i] != b.lL[i] || a.lR[i] != b.lR[i] || a.gLxi[i] != b.gLxi[i] ||
+    if (a.xi[i] != b.xi[i] || a.w[i] != b.w[i] || a.lL[i] != b.lL[i] || a.lR[i] != b.lR[i] || a.gLxi[i] != b.gLxi[i] ||
         a.gRxi[i] != b.gRxi[i] || a.lLD[i] != b.lLD[i] || a.lRD[i] != b.lRD[i])
       return false;
     for (int k = 0; k < n; ++k)
@@ -197,7 +203,8 @@ bool same_tables(const HostOps& a, const HostOps& b) {
 
 // Rebuild the instance table, the groups and their tile lists.
 int rebuild(frg_batch* b) {
-  std::vector<BatchInst> insts(b->cap);
+  std::vector<BatchInst>& insts = b->h_insts;
+  insts.assign(b->cap, BatchInst{});
   for (int i = 0; i < b->cap; ++i) insts[i] = inst_of(b->slot[i]);
   int rc = bcheck(b, cudaMemcpyAsync(b->d_insts, insts.data(), sizeof(BatchInst) * b->cap,
                                      cudaMemcpyHostToDevice, b->ctx->stream), "batch instances");
@@ -223,7 +230,7 @@ int rebuild(frg_batch* b) {
     if (!solo)
       for (auto& g : b->groups)
         if (!g.solo && g.dim == s->dim && g.np == s->np && g.flux == flux && g.av == av && g.variant == variant &&
-            same_tables(g.ops, s->ops)) {
+            g.hook == s->post_step_id && same_tables(g.ops, s->ops)) {
           grp = &g;
           break;
         }
@@ -244,6 +251,9 @@ int rebuild(frg_batch* b) {
       grp->av = av;
       grp->variant = variant;
       grp->solo = solo;
+      grp->hook = s->post_step_id;
+      grp->tx = tx;
+      grp->ty = ty;
       grp->ops = s->ops;
     }
     grp->members.push_back(i);
@@ -308,7 +318,9 @@ int enqueue_group_step(frg_batch* b, const frg_batch::Group& g, cudaStream_t st)
       if (e) return bcheck(b, (cudaError_t)e, "solo stage launch");
     }
     batch_end_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
-    return bcheck(b, cudaGetLastError(), "batch control kernels");
+    const int rc = bcheck(b, cudaGetLastError(), "batch control kernels");
+    // post_step! of a completed step (SSP_RK3.jl:162), as a single solve runs it
+    return rc ? rc : enqueue_post_step_on(b->slot[g.members[0]], false, st);
   }
   for (int stage = 1; stage <= 3; ++stage) {
     const int e = g.dim == 2 ? launch_batch2d(&g.ops, g.flux, g.av, g.variant, b->d_insts, g.d_tiles(),
@@ -318,7 +330,17 @@ int enqueue_group_step(frg_batch* b, const frg_batch::Group& g, cudaStream_t st)
     if (e) return bcheck(b, (cudaError_t)e, "batched stage launch");
   }
   batch_end_kernel<<<nb, 128, 0, st>>>(b->d_insts, g.d_members(), m);
-  return bcheck(b, cudaGetLastError(), "batch control kernels");
+  int rc = bcheck(b, cudaGetLastError(), "batch control kernels");
+  if (rc || !g.hook) return rc;
+  // post_step! of the members whose step completed (SSP_RK3.jl:162), then the
+  // element viscosity and CFL wave speed of their limited states
+  int e = enqueue_batch_post_step(g.ops, g.tx, g.ty, b->d_insts, g.d_tiles(), (int)g.tiles.size(), st);
+  if (!e)
+    e = g.dim == 2 ? launch_batch2d(&g.ops, g.flux, g.av, g.variant, b->d_insts, g.d_tiles(), (int)g.tiles.size(),
+                                    0, kModePrime, st)
+                   : launch_batch1d(&g.ops, g.flux, g.av, b->d_insts, g.d_tiles(), (int)g.tiles.size(), 0,
+                                    kModePrime, st);
+  return e ? bcheck(b, (cudaError_t)e, "batched post-step hook") : FRG_OK;
 }
 
 // `rounds` rounds of every group (group g takes rounds * reps_g steps); the
@@ -516,7 +538,6 @@ int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixe
   if (!b || i < 0 || i >= b->cap || !b->slot[i]) return FRG_ERR_INVALID_ARG;
   frg_solve* s = b->slot[i];
   if (!s->have_state) return set_err(b->ctx, FRG_ERR_STATE, "no state uploaded");
-  if (s->post_step_id) return set_err(b->ctx, FRG_ERR_UNSUPPORTED_HOOK, "batched instances run no post-step hook");
   if (max_steps < 1 || (!(fixed_dt > 0.0) && !(cfl > 0.0))) return set_err(b->ctx, FRG_ERR_INVALID_ARG, "run");
   cudaSetDevice(b->ctx->device);
   int rc = make_current_canonical(s);
@@ -524,6 +545,11 @@ int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixe
   init_run_scalars(s, t_final, cfl, fixed_dt, max_steps);
   if ((rc = push_scalars(s))) return rc;
   if ((rc = prime(s, 0, true))) return rc;  // eps of the state, CFL wave speed
+  // a hook selected after the last rebuild regroups the instance
+  const BatchInst I = inst_of(s);
+  if (i >= (int)b->h_insts.size() || b->h_insts[i].hook != I.hook ||
+      b->h_insts[i].hook_params[0] != I.hook_params[0] || b->h_insts[i].hook_params[1] != I.hook_params[1])
+    b->dirty = true;
   b->running[i] = 1;
   return FRG_OK;
 }
@@ -545,7 +571,7 @@ int frg_batch_run(frg_batch* b, int64_t max_steps, frg_result* results, int* n_r
   int nodes = 0;
   for (auto& g : b->groups) {
     work += g.ndof * (size_t)g.reps;
-    nodes += 5 * g.reps;
+    nodes += (g.hook ? 7 : 5) * g.reps;
   }
   int K = work > 4000000 ? 4 : (work > 400000 ? 8 : 16);
   while (K > 1 && K * nodes > 600) K /= 2;

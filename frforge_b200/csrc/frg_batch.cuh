@@ -9,7 +9,9 @@
 
 namespace frg {
 
-// Stage buffers of an instance for stage `stage` (or the prime pass).
+// Stage buffers of an instance for stage `stage` (or the prime pass, which
+// the batched kernels run only as the post-step pass of a hooked group, on the
+// instances whose step just completed).
 FRG_DEV StageBufs batch_bufs(const BatchInst& I, int stage, int mode) {
   StageBufs b{};
   b.sc = I.sc;
@@ -85,6 +87,7 @@ __global__ void __launch_bounds__(NTHR, MINB)
   const BatchTile t = tiles[blockIdx.x];
   const BatchInst* I = &insts[t.inst];
   if (mode == kModeStage && stage == 3 && I->rk2) return;  // SSP-RK2 has two stages
+  if (mode == kModePrime && !I->sc->stepped_ok) return;    // post-step pass: completed steps only
   copy_to_smem(&sM, &I->M2);
   copy_to_smem(&sP, &I->P);
   if (threadIdx.x == 0) sB = batch_bufs(*I, stage, mode);
@@ -102,6 +105,7 @@ __global__ void __launch_bounds__(256)
   const BatchTile t = tiles[blockIdx.x];
   const BatchInst* I = &insts[t.inst];
   if (mode == kModeStage && stage == 3 && I->rk2) return;
+  if (mode == kModePrime && !I->sc->stepped_ok) return;
   copy_to_smem(&sM, &I->M1);
   copy_to_smem(&sP, &I->P);
   if (threadIdx.x == 0) sB = batch_bufs(*I, stage, mode);

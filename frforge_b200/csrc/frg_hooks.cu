@@ -106,13 +106,9 @@ __device__ void zs_element(double* u, size_t n, size_t base, int npts, const dou
       }
 }
 
-// one thread per element; `force` ignores the step's completion flag
-__global__ void zs_limiter_2d(double* u, const Mesh2Dev M, Weights W, int np, double g1, double er, double ep,
-                              DevScalars* sc, int force) {
-  if (!force && !(sc && sc->stepped_ok)) return;
-  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;  // the prime pass recomputes it
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= M.nel) return;
+// Zhang-Shu scaling of 2D element e (quadrature weights w_i w_j |J|)
+__device__ void zs_element_2d(double* u, const Mesh2Dev& M, const Weights& W, int np, double g1, double er,
+                              double ep, int e) {
   if (M.solid && M.solid[e]) return;
   const int np2 = np * np;
   const size_t n = (size_t)M.nel * np2, base = (size_t)e * np2;
@@ -125,31 +121,71 @@ __global__ void zs_limiter_2d(double* u, const Mesh2Dev M, Weights W, int np, do
   zs_element<4>(u, n, base, np2, ww, g1, er, ep);
 }
 
-__global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, double g1, double er, double ep,
-                              DevScalars* sc, int force) {
-  if (!force && !(sc && sc->stepped_ok)) return;
-  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= M.nel) return;
+__device__ void zs_element_1d(double* u, const Mesh1Dev& M, const Weights& W, int np, double g1, double er,
+                              double ep, int e) {
   const size_t n = (size_t)M.nel * np, base = (size_t)e * np;
   double ww[kMaxNp];
   for (int k = 0; k < np; ++k) ww[k] = W.w[k] * M.J[e];
   zs_element<3>(u, n, base, np, ww, g1, er, ep);
 }
 
-}  // namespace
+// one thread per element; `force` ignores the step's completion flag
+__global__ void zs_limiter_2d(double* u, const Mesh2Dev M, Weights W, int np, double g1, double er, double ep,
+                              DevScalars* sc, int force) {
+  if (!force && !(sc && sc->stepped_ok)) return;
+  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;  // the prime pass recomputes it
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  zs_element_2d(u, M, W, np, g1, er, ep, e);
+}
 
-// Enqueue the post-step hook of a solve on its stream (no-op without one):
-// the hook kernel, then the prime pass of the limited state.  force: run even
-// if no step just completed.
-int enqueue_post_step(frg_solve* s, bool force) {
-  if (s->post_step_id != kHookPositivity) return FRG_OK;
+__global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, double g1, double er, double ep,
+                              DevScalars* sc, int force) {
+  if (!force && !(sc && sc->stepped_ok)) return;
+  if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  zs_element_1d(u, M, W, np, g1, er, ep, e);
+}
+
+// Batched groups: one CTA per TX x TY tile of the group's tile list, one
+// thread per element of the tile; instances whose step did not complete, or
+// that carry no hook, are left alone.  The CTA of an instance's first tile
+// clears its CFL wave speed, which the group's prime pass recomputes.
+__global__ void zs_limiter_batch(const BatchInst* __restrict__ insts, const BatchTile* __restrict__ tiles,
+                                 Weights W, int np, int tx, int ty) {
+  const BatchTile t = tiles[blockIdx.x];
+  const BatchInst& I = insts[t.inst];
+  if (I.hook != kHookPositivity || !(I.sc && I.sc->stepped_ok)) return;
+  if (t.x0 == 0 && t.y0 == 0 && threadIdx.x == 0) I.sc->lam_bits = 0ull;
+  const double er = I.hook_params[0], ep = I.hook_params[1];
+  for (int k = threadIdx.x; k < tx * ty; k += blockDim.x) {
+    const int x = t.x0 + k % tx, y = t.y0 + k / tx;
+    if (I.dim == 2) {
+      if (x < I.M2.nx && y < I.M2.ny) zs_element_2d(I.U[0], I.M2, W, np, I.P.g1, er, ep, y * I.M2.nx + x);
+    } else if (x < I.M1.nel) {
+      zs_element_1d(I.U[0], I.M1, W, np, I.P.g1, er, ep, x);
+    }
+  }
+}
+
+Weights weights_of(const HostOps& ops) {
   Weights W;
   std::memset(&W, 0, sizeof(W));
-  for (int i = 0; i < s->np; ++i) W.w[i] = s->ops.w[i];
+  for (int i = 0; i < ops.np; ++i) W.w[i] = ops.w[i];
+  return W;
+}
+
+}  // namespace
+
+// Enqueue the post-step hook of a solve on stream `st` (no-op without one):
+// the hook kernel, then the prime pass of the limited state.  force: run even
+// if no step just completed.
+int enqueue_post_step_on(frg_solve* s, bool force, cudaStream_t st) {
+  if (s->post_step_id != kHookPositivity) return FRG_OK;
+  const Weights W = weights_of(s->ops);
   const int threads = 128, blocks = (s->nel + threads - 1) / threads;
   const double er = s->post_step_params[0], ep = s->post_step_params[1];
-  cudaStream_t st = s->ctx->stream;
   if (s->dim == 2)
     zs_limiter_2d<<<blocks, threads, 0, st>>>(s->U[0], s->L2.mesh, W, s->np, s->L2.phys.g1, er, ep, s->sc,
                                                force ? 1 : 0);
@@ -158,7 +194,15 @@ int enqueue_post_step(frg_solve* s, bool force) {
                                                force ? 1 : 0);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return rt::cuda_err(s->ctx, e, "post-step hook");
-  return rt::prime(s, 0, true);
+  return rt::prime_on(s, 0, true, st);
+}
+int enqueue_post_step(frg_solve* s, bool force) { return enqueue_post_step_on(s, force, s->ctx->stream); }
+
+int enqueue_batch_post_step(const HostOps& ops, int tx, int ty, const BatchInst* insts, const BatchTile* tiles,
+                            int ntiles, cudaStream_t st) {
+  if (ntiles < 1) return (int)cudaSuccess;
+  zs_limiter_batch<<<ntiles, 128, 0, st>>>(insts, tiles, weights_of(ops), ops.np, tx, ty);
+  return (int)cudaGetLastError();
 }
 
 }  // namespace frg

@@ -154,6 +154,9 @@ struct BatchInst {
   DevScalars* sc;
   int rk2;
   int dim;
+  int hook;              // post-step hook id (kHookNone: none)
+  int hook_pad;
+  double hook_params[2];  // kHookPositivity: eps_rho, eps_p
 };
 // A tile of one instance: first element (x0, y0) of a TX x TY tile.
 struct BatchTile {

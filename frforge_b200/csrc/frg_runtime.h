@@ -58,13 +58,21 @@ int push_scalars(frg_solve* s);
 int pull_scalars(frg_solve* s);
 int launch(frg_solve* s, const StageBufs& b);
 int prime(frg_solve* s, int buf, bool want_lambda);
+int prime_on(frg_solve* s, int buf, bool want_lambda, cudaStream_t st);
 int finish_run(frg_solve* s);
 int make_current_canonical(frg_solve* s);
 void init_run_scalars(frg_solve* s, double t_final, double cfl, double fixed_dt, int64_t max_steps);
 StageBufs stage_bufs(const frg_solve* s, int stage, bool want_lambda);
 }  // namespace rt
-// post-step hook of a solve and the prime pass of its result (frg_hooks.cu)
+// post-step hook of a solve and the prime pass of its result (frg_hooks.cu),
+// on the solve's stream or on `st`
 int enqueue_post_step(frg_solve* s, bool force);
+int enqueue_post_step_on(frg_solve* s, bool force, cudaStream_t st);
+// post-step hook of the instances of a batched group whose step completed,
+// one CTA per TX x TY tile of the group's tile list (frg_hooks.cu); the
+// caller follows it with the group's prime pass
+int enqueue_batch_post_step(const HostOps& ops, int tx, int ty, const BatchInst* insts, const BatchTile* tiles,
+                            int ntiles, cudaStream_t st);
 __global__ void step_begin_kernel(DevScalars* sc);
 __global__ void step_end_kernel(DevScalars* sc, int nstages);
 }  // namespace frg

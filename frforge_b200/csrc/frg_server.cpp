@@ -34,6 +34,9 @@ struct Request {
   double* u_out;
   size_t bytes;
   size_t ndof;
+  int hook_slot, hook_id;  // post-step hook applied at admission (id 0: none)
+  int hook_nparams;
+  double hook_params[2];
 };
 
 struct Outcome {
@@ -106,6 +109,8 @@ int admit(frg_server* s) {
     frg_solve* sv = nullptr;
     frg_batch_get_solve(s->batch, slot, &sv);
     rc = q.u0 ? frg_upload_state(sv, q.u0, q.ndof, q.t0) : frg_set_initial_condition(sv, &q.ic);
+    if (!rc && q.hook_id)
+      rc = frg_solve_set_hook(sv, q.hook_slot, q.hook_id, q.hook_params, q.hook_nparams);
     if (!rc) rc = frg_batch_start(s->batch, slot, q.t_final, q.cfl, q.fixed_dt, q.max_steps);
     if (rc) {
       frg_batch_remove(s->batch, slot);
@@ -188,6 +193,38 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
   Request& q = s->queue.back();
   q.u0 = nullptr;
   q.ic = *ic;
+  return FRG_OK;
+}
+
+// Hook of a queued request, validated against the registry now and applied
+// to its solve at admission.
+int frg_server_set_hook(frg_server* s, int64_t id, int slot, int hook_id, const double* params, int nparams) {
+  if (!s) return FRG_ERR_INVALID_ARG;
+  Request* q = nullptr;
+  for (Request& r : s->queue)
+    if (r.id == id) q = &r;
+  if (!q) {
+    if (s->outcome.count(id)) return set_err(s->ctx, FRG_ERR_STATE, "set_hook: request already admitted");
+    return FRG_ERR_INVALID_ARG;
+  }
+  if (slot != FRG_HOOK_POST_STEP) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook slot");
+  if (hook_id != 0) {
+    int maxp = -1;
+    for (int i = 0, n = frg_hook_count(); i < n; ++i) {
+      int sl = -1, hid = -1, np = 0;
+      frg_hook_info(i, nullptr, &sl, &hid, &np);
+      if (sl == slot && hid == hook_id) maxp = np;
+    }
+    if (maxp < 0) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook implementation");
+    if (nparams < 0 || nparams > maxp || nparams > 2 || (nparams > 0 && !params))
+      return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters");
+    for (int k = 0; k < nparams; ++k)
+      if (!(params[k] > 0.0)) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters must be > 0");
+  }
+  q->hook_slot = slot;
+  q->hook_id = hook_id;
+  q->hook_nparams = hook_id ? nparams : 0;
+  for (int k = 0; k < q->hook_nparams; ++k) q->hook_params[k] = params[k];
   return FRG_OK;
 }
 

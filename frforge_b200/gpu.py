@@ -157,6 +157,27 @@ def diagnostics_of(handle, ctx, exact: str, t_exact: float, c: int, ref_ptr: int
             "l2_error": d.l2_error, "t": d.t}
 
 
+def method_hooks(method: Optional[AbstractCapturingMethod]):
+    """The device hooks a method selects: [(slot id, hook id, params)] from its
+    gpu_spec()["hooks"] {slot name: (implementation name, params)}, resolved
+    through the registry (frg_hook_lookup)."""
+    out = []
+    for slot, (name, params) in (method or NullCapturing()).gpu_spec().get("hooks", {}).items():
+        sl, hid = C.c_int(), C.c_int()
+        L.check(L.load().frg_hook_lookup(name.encode(), C.byref(sl), C.byref(hid)), None, "frg_hook_lookup")
+        if sl.value != L.HOOK_SLOT[slot]:
+            raise ValueError(f"{name} implements another hook slot")
+        out.append((sl.value, hid.value, np.ascontiguousarray(np.asarray(params, dtype=np.float64))))
+    return out
+
+
+def set_solve_hooks(handle, ctx: "Context", method: Optional[AbstractCapturingMethod]) -> None:
+    """Select on solve `handle` the device hooks of `method` (frg_solve_set_hook)."""
+    for sl, hid, arr in method_hooks(method):
+        L.check(L.load().frg_solve_set_hook(handle, sl, hid, L.dptr(arr) if arr.size else None, int(arr.size)),
+                ctx.handle, "frg_solve_set_hook")
+
+
 class GpuSolve:
     """A device-resident solve (frg_solve): descriptor, state buffers, graphs."""
 
@@ -173,8 +194,7 @@ class GpuSolve:
         info = self.info()
         self.ndof, self.nel = info["ndof"], info["nel"]
         # device implementations of the hooks the method overrides
-        for slot, (name, params) in (method or NullCapturing()).gpu_spec().get("hooks", {}).items():
-            self.set_hook(slot, name, params)
+        set_solve_hooks(self.handle, self.ctx, method)
 
     def set_hook(self, slot: str, name: str, params=()) -> None:
         """Select the device implementation `name` of hook `slot`

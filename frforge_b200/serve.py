@@ -15,8 +15,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import _lib as L
-from .batch import _refuse_hooks
-from .gpu import Context, default_context, make_desc
+from .gpu import Context, default_context, make_desc, method_hooks
 from .methods import AbstractCapturingMethod
 
 
@@ -53,8 +52,8 @@ class Server:
         """Queue ``integrate_(state, eq, method, t_final; cfl, dt, max_steps)``;
         returns the request id.  want_state=False: only the device-side
         diagnostics of the final state are returned, not the state."""
-        _refuse_hooks(method)
         d, keep = make_desc(state, eq, method, time)
+        hooks = method_hooks(method)
         u0 = np.ascontiguousarray(np.asarray(state.u, dtype=np.float64).ravel(order="F"))
         out = np.empty_like(u0) if want_state else None
         rid = C.c_int64()
@@ -63,6 +62,7 @@ class Server:
                                              L.dptr(out) if want_state else None, C.byref(rid)),
                   "frg_server_submit")
         self._req[rid.value] = (d, keep, u0, out, state.u.shape)
+        self._set_hooks(rid.value, hooks)
         return rid.value
 
     def submit_ic(self, state, eq, ic: dict, method: Optional[AbstractCapturingMethod] = None,
@@ -71,8 +71,8 @@ class Server:
         """As submit, with the initial state evaluated on the device at
         admission from the case IC ``ic`` (keyword arguments of
         frforge_b200._lib.make_ic); ``state`` gives the mesh and scheme only."""
-        _refuse_hooks(method)
         d, keep = make_desc(state, eq, method, time)
+        hooks = method_hooks(method)
         c_ic = L.make_ic(**ic)
         out = np.empty(int(np.prod(state.u.shape))) if want_state else None
         rid = C.c_int64()
@@ -81,7 +81,18 @@ class Server:
                                                 L.dptr(out) if want_state else None, C.byref(rid)),
                   "frg_server_submit_ic")
         self._req[rid.value] = (d, keep, None, out, state.u.shape)
+        self._set_hooks(rid.value, hooks)
         return rid.value
+
+    def _set_hooks(self, rid: int, hooks) -> None:
+        """Attach the method's device hooks to the queued request (applied at
+        admission, frg_server_set_hook); a refused hook cancels the request."""
+        for sl, hid, arr in hooks:
+            code = L.load().frg_server_set_hook(self.handle, int(rid), sl, hid, L.dptr(arr) if arr.size else None,
+                                                int(arr.size))
+            if code:
+                L.load().frg_server_cancel(self.handle, int(rid))
+                self._chk(code, "frg_server_set_hook")
 
     def cancel(self, rid: int) -> None:
         self._chk(L.load().frg_server_cancel(self.handle, int(rid)), "frg_server_cancel")

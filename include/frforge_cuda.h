@@ -439,7 +439,10 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
         Zhang & Shu (J. Comput. Phys. 229, 2010) toward the element mean,
         density >= params[0], pressure >= params[1] (default 1e-13 each);
         element integrals are unchanged.
-   Batched instances run no hooks (frg_batch_start refuses them). */
+   Batched instances run their hooks too: set one on the slot's solve
+   (frg_batch_get_solve) before frg_batch_start, or on a queued request with
+   frg_server_set_hook; the batch groups instances by hook and steps them
+   to the same results as a single solve. */
 enum { FRG_HOOK_POST_STEP = 0 };
 int frg_hook_count(void);
 int frg_hook_info(int index, const char** name, int* slot, int* id, int* nparams);
@@ -449,6 +452,11 @@ int frg_hook_lookup(const char* name, int* slot, int* id);
 int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams);
 /* Apply the post-step hook once to the current state (host-driven loops). */
 int frg_apply_post_step(frg_solve* s);
+/* Select hook `id` of `slot` for a request that is still queued (id 0
+   removes it); applied to the request's solve at admission.  FRG_ERR_STATE
+   once the request was admitted or completed. */
+int frg_server_set_hook(frg_server* s, int64_t request_id, int slot, int id, const double* params,
+                        int nparams);
 
 #ifdef __cplusplus
 }

@@ -1,13 +1,18 @@
 """Device hook registry: the Zhang-Shu post-step kernel against its host
 restatement on identical states (1D, 2D affine, 2D wavy), and its place in
 the device time loop against a host-driven loop of single steps with the
-host hook in between."""
+host hook in between.  Batched and served instances run the hook after each
+of their completed steps: bit-identical to the instance alone in a batch and
+within 1e-10 of the single-solve path (bit-identical for solo groups)."""
 import numpy as np
 import pytest
 
 import frforge_b200 as F
+from frforge_b200 import _lib as L
 from frforge_b200.batch import Batch
+from frforge_b200.gpu import set_solve_hooks
 from frforge_b200.limiters import zhang_shu_limit_
+from frforge_b200.serve import Server
 
 from pairs import four_quadrant_state, pair_1d, pair_2d, rel_linf
 
@@ -94,9 +99,146 @@ def test_time_loop_matches_host_driven_steps():
     assert np.min(u_dev[..., 0]) >= er * (1 - 1e-12) and np.min(u_plain[..., 0]) < er
 
 
-def test_batch_refuses_hook_methods():
-    orc, state, _ = pair_2d(p=2, nx=4, ny=4)
+def _hooked_cases():
+    """(state, eq, hooked method, plain method, run) of the batch tests: the
+    thresholds sit just below each initial state's minima, so the hook clips
+    the undershoots at the discontinuities every step."""
+    eq2, eq1 = F.Euler2D(1.4), F.Euler1D(1.4)
+    out = []
+    for k, (kw, scale) in enumerate([
+            (dict(p=3, nx=16, ny=16, flux="hllc"), 0.25),
+            (dict(p=2, nx=12, ny=10, flux="rusanov", time="ssp_rk2"), 0.25),
+            (dict(p=2, nx=10, ny=10, flux="hllc", wavy=1), 0.2)]):
+        orc, state, _ = pair_2d(method="persson", bcs=("transmissive",) * 4, **kw)
+        u0 = four_quadrant_state(orc, seed=60 + k, jump_scale=scale)
+        state.u[...] = u0
+        state.t = 0.0
+        er = 0.98 * float(np.min(u0[..., 0]))
+        ep = 0.98 * float(np.min(eq2.pressure(u0)))
+        out.append((state, eq2, F.PositivityPreservingPersson(eps_rho=er, eps_p=ep), F.PerssonAVMethod(),
+                    dict(t_final=1.0, cfl=0.1, max_steps=10)))
+    orc, state, _ = pair_1d(p=3, nel=48, method="persson")
+    orc.ic_sod()
+    state.u[...] = orc.u
+    state.t = 0.0
+    out.append((state, eq1, F.PositivityPreservingPersson(eps_rho=0.124, eps_p=0.099), F.PerssonAVMethod(),
+                dict(t_final=1.0, cfl=0.15, max_steps=40)))
+    return out
+
+
+def _single(state, eq, m, run):
+    s = F.GpuSolve(state, eq, m)
+    s.upload(state.u, 0.0)
+    r = s.advance(run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    u, t = s.download()
+    s.close()
+    return r, u, t
+
+
+def _alone(state, eq, m, run):
     b = Batch(capacity=1)
-    with pytest.raises(F.UnsupportedHookError):
-        b.add(state, F.Euler2D(1.4), F.PositivityPreservingPersson())
+    i = b.add(state, eq, m)
+    b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    r = b.run()[i]
+    u, t = b.download(i)
     b.close()
+    return r, u, t
+
+
+def test_batch_runs_post_step_hook_like_a_single_solve():
+    # hooked instances (2D affine RK3/RK2, 2D wavy, 1D) beside their unhooked
+    # twins in one batch: each ends bit-identical to itself alone in a batch,
+    # within 1e-10 of the single-solve path with the hook, and away from the
+    # unhooked run
+    cases = _hooked_cases()
+    b = Batch(capacity=2 * len(cases))
+    slots = []
+    for state, eq, mh, mp, run in cases:
+        for m in (mh, mp):
+            i = b.add(state, eq, m)
+            b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+            slots.append(i)
+    res = b.run()
+    for k, (state, eq, mh, mp, run) in enumerate(cases):
+        ih, ip = slots[2 * k], slots[2 * k + 1]
+        uh, th = b.download(ih)
+        up, _ = b.download(ip)
+        r_alone, u_alone, t_alone = _alone(state, eq, mh, run)
+        assert res[ih] == r_alone and th == t_alone and np.array_equal(uh, u_alone), k
+        r_one, u_one, t_one = _single(state, eq, mh, run)
+        assert res[ih]["status"] == r_one["status"] == "max_steps", k
+        assert res[ih]["n_steps"] == r_one["n_steps"], k
+        assert th == pytest.approx(t_one, rel=1e-13), k
+        assert rel_linf(uh, u_one) <= 1e-10, k
+        # the hook acted: the plain run breaks a floor that the hooked run
+        # keeps, and the two runs differ
+        assert np.min(uh[..., 0]) >= mh.eps_rho * (1 - 1e-12), k
+        assert np.min(eq.pressure(uh)) >= mh.eps_p * (1 - 1e-9), k
+        assert np.min(up[..., 0]) < mh.eps_rho or np.min(eq.pressure(up)) < mh.eps_p, k
+        assert rel_linf(uh, up) > 1e-8, k
+    b.close()
+
+
+def test_solo_group_runs_post_step_hook():
+    # 200^2 P=3 fills a wave of batched tiles and runs solo inside the batch,
+    # through the single-solve kernels and hook: bit-identical to frg_advance
+    orc, state, _ = pair_2d(p=3, nx=200, ny=200, flux="hllc", method="persson", bcs=("transmissive",) * 4)
+    u0 = four_quadrant_state(orc, seed=71, jump_scale=0.25)
+    state.u[...] = u0
+    state.t = 0.0
+    eq = F.Euler2D(1.4)
+    m = F.PositivityPreservingPersson(eps_rho=0.98 * float(np.min(u0[..., 0])),
+                                      eps_p=0.98 * float(np.min(eq.pressure(u0))))
+    run = dict(t_final=1.0, cfl=0.1, max_steps=6)
+    r_one, u_one, t_one = _single(state, eq, m, run)
+    b = Batch(capacity=2)
+    i = b.add(state, eq, m)
+    b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    r = b.run()[i]
+    u, t = b.download(i)
+    b.close()
+    assert r["status"] == r_one["status"] and r["n_steps"] == r_one["n_steps"] == 6
+    assert t == t_one and np.array_equal(u, u_one)
+
+
+def test_hook_selected_between_runs_regroups_the_instance():
+    # a plain run, then the same slot restarted after a hook was selected on
+    # its solve: the second run is the hooked one
+    state, eq, mh, mp, run = _hooked_cases()[0]
+    b = Batch(capacity=2)
+    i = b.add(state, eq, mp)
+    b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    b.run()
+    b.upload(i, state.u, 0.0)
+    set_solve_hooks(b._solve(i), b.ctx, mh)
+    b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    r = b.run()[i]
+    u, t = b.download(i)
+    b.close()
+    r_alone, u_alone, t_alone = _alone(state, eq, mh, run)
+    assert r == r_alone and t == t_alone and np.array_equal(u, u_alone)
+
+
+def test_server_runs_post_step_hook():
+    cases = _hooked_cases()
+    srv = Server(slots=3, steps_per_pump=4)
+    ids = []
+    for state, eq, mh, mp, run in cases:
+        ids.append(srv.submit(state, eq, mh, t_final=run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"]))
+    srv.drain()
+    for rid, (state, eq, mh, mp, run) in zip(ids, cases):
+        res = srv.result(rid)
+        r_alone, u_alone, t_alone = _alone(state, eq, mh, run)
+        assert res["status"] == r_alone["status"] and res["n_steps"] == r_alone["n_steps"]
+        assert res["t"] == t_alone and np.array_equal(res["u"], u_alone)
+    # a hook for an admitted request, or an unknown one, is refused
+    state, eq, mh, mp, run = cases[0]
+    rid = srv.submit(state, eq, mp, t_final=run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    lib = L.load()
+    par, bad = np.array([1e-3, 1e-3]), np.array([-1e-3, 1e-3])
+    assert lib.frg_server_set_hook(srv.handle, rid, 0, 7, L.dptr(par), 2) == L.FRG_ERR_UNSUPPORTED_HOOK
+    assert lib.frg_server_set_hook(srv.handle, rid, 0, 1, L.dptr(bad), 2) == L.FRG_ERR_INVALID_ARG
+    srv.pump()
+    assert lib.frg_server_set_hook(srv.handle, rid, 0, 1, L.dptr(par), 2) == L.FRG_ERR_STATE
+    srv.drain()
+    srv.close()
