@@ -242,3 +242,48 @@ def test_server_runs_post_step_hook():
     assert lib.frg_server_set_hook(srv.handle, rid, 0, 1, L.dptr(par), 2) == L.FRG_ERR_STATE
     srv.drain()
     srv.close()
+
+
+def test_multirate_batch_with_hooks_matches_alone():
+    # multirate scheduling gives the groups different step counts per round;
+    # hooked and plain instances still end as they do alone in a batch
+    cases = _hooked_cases()
+    b = Batch(capacity=2 * len(cases))
+    b.set_multirate(True)
+    slots = []
+    for state, eq, mh, mp, run in cases:
+        for m in (mh, mp):
+            i = b.add(state, eq, m)
+            b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+            slots.append((i, state, eq, m, run))
+    res = b.run()
+    for i, state, eq, m, run in slots:
+        r_alone, u_alone, t_alone = _alone(state, eq, m, run)
+        u, t = b.download(i)
+        assert res[i] == r_alone and t == t_alone and np.array_equal(u, u_alone), i
+    b.close()
+
+
+def test_served_device_ic_with_hook_matches_alone():
+    # a hooked request admitted with its initial state evaluated on the device
+    orc, state, _ = pair_2d(p=2, nx=16, ny=16, flux="hllc", method="persson", bcs=("transmissive",) * 4)
+    eq = F.Euler2D(1.4)
+    ic = dict(kind="four_quadrant", prim=[(1.0, 0.0, 0.0, 1.0), (0.5, 0.6, 0.0, 0.4), (0.15, 0.6, 0.6, 0.05),
+                                           (0.3, 0.0, 0.6, 0.2)], x0=0.5, y0=0.5)
+    m = F.PositivityPreservingPersson(eps_rho=0.14, eps_p=0.045)
+    run = dict(t_final=1.0, cfl=0.1, max_steps=15)
+    srv = Server(slots=2, steps_per_pump=4)
+    rid = srv.submit_ic(state, eq, ic, m, t_final=run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    srv.drain()
+    res = srv.result(rid)
+    srv.close()
+    b = Batch(capacity=1)
+    i = b.add(state, eq, m)
+    b.set_initial_condition(i, **ic)
+    b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+    r = b.run()[i]
+    u, t = b.download(i)
+    b.close()
+    assert res["status"] == r["status"] == "max_steps" and res["n_steps"] == r["n_steps"] == 15
+    assert res["t"] == t and np.array_equal(res["u"], u)
+    assert np.min(u[..., 0]) >= 0.14 * (1 - 1e-12)
