@@ -80,3 +80,16 @@ def test_registry_lists_the_device_hook():
 
     hooks = L.device_hooks()
     assert hooks["positivity_zhang_shu"] == (L.HOOK_SLOT["post_step"], 1, 2)
+
+
+def test_method_hooks_resolve_through_the_registry():
+    # what Batch.add and Server.submit attach to an instance: slot and id from
+    # the registry, the method's parameters as given
+    from frforge_b200 import _lib as L
+    from frforge_b200.gpu import method_hooks
+
+    (sl, hid, par), = method_hooks(F.PositivityPreservingPersson(eps_rho=2e-3, eps_p=5e-4))
+    assert (sl, hid) == (L.HOOK_SLOT["post_step"], 1)
+    assert par.dtype == np.float64 and list(par) == [2e-3, 5e-4]
+    assert method_hooks(F.PerssonAVMethod()) == []
+    assert method_hooks(None) == []
