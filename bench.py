@@ -199,12 +199,13 @@ def max_over_ranks(ms: float, world: int, device: str) -> float:
     return float(t.item())
 
 
-def advance_launches(steps: int, ndof: int) -> int:
+def advance_launches(steps: int, ndof: int, loop1d: bool = False) -> int:
     """Kernels one frg_advance of `steps` SSP-RK3 steps launches: the prime
     pass, then graphs of K steps (K by state size, as run_steps picks it) of
-    five kernels per step (begin, three stages, end)."""
+    five kernels per step (begin, three stages, end); a 1D solve of at most 8
+    tiles instead runs K steps per launch of the cluster loop kernel."""
     k = 4 if ndof > 4e6 else (16 if ndof > 2e5 else 64)
-    return 1 + -(-steps // k) * 5 * k
+    return 1 + -(-steps // k) * (1 if loop1d else 5 * k)
 
 
 def replica_rate(world: int, steps: int, ndof: int, ms_max: float) -> float:
@@ -390,7 +391,7 @@ def run_c1(args):
         "e2e": {"value": steps / (ms_e2e * 1e-3), "unit": "steps/s", "h2d_bytes_per_step": ndof * 8 / steps,
                 "d2h_bytes_per_step": ndof * 8 / steps},
         "clocks": clk.summary(),
-        "gpu_launches": advance_launches(steps, ndof),
+        "gpu_launches": advance_launches(steps, ndof, loop1d=True),
     }
     print(json.dumps(line))
     return 0

@@ -30,6 +30,11 @@ int launch_stage1d_np3(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np4(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np5(const Launch1D&, const StageBufs&, cudaStream_t);
 int launch_stage1d_np6(const Launch1D&, const StageBufs&, cudaStream_t);
+int launch_loop1d_np2(const Launch1D&, const Loop1DBufs&, DevScalars*, int, cudaStream_t);
+int launch_loop1d_np3(const Launch1D&, const Loop1DBufs&, DevScalars*, int, cudaStream_t);
+int launch_loop1d_np4(const Launch1D&, const Loop1DBufs&, DevScalars*, int, cudaStream_t);
+int launch_loop1d_np5(const Launch1D&, const Loop1DBufs&, DevScalars*, int, cudaStream_t);
+int launch_loop1d_np6(const Launch1D&, const Loop1DBufs&, DevScalars*, int, cudaStream_t);
 int stage2d_variants_np2();
 int stage2d_variants_np3();
 int stage2d_variants_np4();
@@ -55,6 +60,16 @@ int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream) {
     case 4: return launch_stage2d_np4(L, b, st);
     case 5: return launch_stage2d_np5(L, b, st);
     case 6: return launch_stage2d_np6(L, b, st);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+int launch_loop1d(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+  switch (L.ops->np) {
+    case 2: return launch_loop1d_np2(L, lb, sc, nsteps, st);
+    case 3: return launch_loop1d_np3(L, lb, sc, nsteps, st);
+    case 4: return launch_loop1d_np4(L, lb, sc, nsteps, st);
+    case 5: return launch_loop1d_np5(L, lb, sc, nsteps, st);
+    case 6: return launch_loop1d_np6(L, lb, sc, nsteps, st);
   }
   return (int)cudaErrorInvalidValue;
 }
@@ -755,7 +770,15 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
   const double dof_per_step = (double)s->ndof;
   int K = dof_per_step > 4e6 ? 4 : (dof_per_step > 2e5 ? 16 : 64);
   if (!use_graph) K = 1;
-  if (use_graph) {
+  // a hook-free 1D solve of at most kLoop1DMaxTiles tiles: K steps per launch
+  // of one thread-block cluster (loop1d_kernel) instead of a step graph
+  bool loop1d = false;
+  if (use_graph && s->dim == 1 && s->post_step_id == kHookNone) {
+    int tx = 1, ty = 1;
+    batch_tile_shape(1, s->np, 0, &tx, &ty);
+    loop1d = (s->nel + tx - 1) / tx <= kLoop1DMaxTiles;
+  }
+  if (use_graph && !loop1d) {
     // the graph depends only on buffers, tables and the dt mode of the solve
     if (!s->graph || s->graph_steps != K || s->graph_lambda != want_lambda) {
       if (s->graph) {
@@ -782,7 +805,13 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
   if (stage_ms)
     for (int k = 0; k < 6; ++k) cudaEventCreate(&ev[k]);
   for (;;) {
-    if (use_graph) {
+    if (loop1d) {
+      Loop1DBufs lb{};
+      lb.nstages = s->time_scheme == FRG_TIME_SSP_RK2 ? 2 : 3;
+      for (int k = 0; k < lb.nstages; ++k) lb.st[k] = stage_bufs(s, k + 1, want_lambda);
+      const int e = launch_loop1d(s->L1, lb, s->sc, K, s->ctx->stream);
+      if (e) return cuda_err(s->ctx, (cudaError_t)e, "1D loop kernel launch");
+    } else if (use_graph) {
       FRG_CUDA(cudaGraphLaunch(s->graph, s->ctx->stream), "graph launch");
     } else {
       if ((rc = enqueue_step(s, want_lambda, stage_ms ? ev : nullptr))) return rc;

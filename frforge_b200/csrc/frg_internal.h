@@ -200,6 +200,15 @@ struct Launch1D {
   int flux;
   int av;
 };
+// The stage buffers of one SSP-RK step, for the whole-solve 1D loop kernel.
+struct Loop1DBufs {
+  StageBufs st[3];
+  int nstages;
+  int pad;
+};
+// Largest 1D mesh, in tiles, that one thread-block cluster steps by itself
+// (one tile per CTA; 8 is the portable cluster size).
+constexpr int kLoop1DMaxTiles = 8;
 // Returns 0 or a CUDA error code.
 int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream);
 // batched stage launch over a group's tile list (same NP, flux, AV, tables)

@@ -153,6 +153,50 @@ int launch1d_inst(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// nsteps steps of a 1D solve of at most kLoop1DMaxTiles tiles by one cluster
+template <int NP, int FLUX, int AV>
+int loop1d_inst(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+  using S = Smem1D<NP>;
+  auto kern = loop1d_kernel<NP, FLUX, AV>;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    if (e != cudaSuccess) return (int)e;
+    configured = true;
+  }
+  const int ntiles = (L.mesh.nel + S::TX - 1) / S::TX;
+  if (ntiles < 1 || ntiles > kLoop1DMaxTiles) return (int)cudaErrorInvalidValue;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ntiles);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = S::bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = ntiles;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return (int)cudaLaunchKernelEx(&cfg, kern, make_ops<NP>(*L.ops), L.mesh, L.phys, lb, sc, nsteps);
+}
+
+template <int NP>
+int loop1d_np(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+  const bool hllc = L.flux == FRG_FLUX_HLLC;
+  switch (L.av) {
+    case kAvBR0:
+      return hllc ? loop1d_inst<NP, FRG_FLUX_HLLC, kAvBR0>(L, lb, sc, nsteps, st)
+                  : loop1d_inst<NP, FRG_FLUX_RUSANOV, kAvBR0>(L, lb, sc, nsteps, st);
+    case kAvDD:
+      return hllc ? loop1d_inst<NP, FRG_FLUX_HLLC, kAvDD>(L, lb, sc, nsteps, st)
+                  : loop1d_inst<NP, FRG_FLUX_RUSANOV, kAvDD>(L, lb, sc, nsteps, st);
+    default:
+      return hllc ? loop1d_inst<NP, FRG_FLUX_HLLC, kAvNone>(L, lb, sc, nsteps, st)
+                  : loop1d_inst<NP, FRG_FLUX_RUSANOV, kAvNone>(L, lb, sc, nsteps, st);
+  }
+}
+
 template <int NP>
 int launch2d_np(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
   const bool hllc = L.flux == FRG_FLUX_HLLC;
@@ -283,6 +327,10 @@ int variants2d() {
   }                                                                                          \
   int launch_stage1d_np##NPV(const Launch1D& L, const StageBufs& b, cudaStream_t st) {       \
     return launch1d_np<NPV>(L, b, st);                                                       \
+  }                                                                                          \
+  int launch_loop1d_np##NPV(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int n,  \
+                            cudaStream_t st) {                                               \
+    return loop1d_np<NPV>(L, lb, sc, n, st);                                                 \
   }                                                                                          \
   int stage2d_variants_np##NPV() { return variants2d<NPV>(); }                                \
   int launch_batch2d_np##NPV(const HostOps& h, int flux, int av, int variant, const BatchInst* insts, \

@@ -9,6 +9,7 @@
 // element viscosity (:158-177) and the CFL wave speed (SSP_RK3.jl:8-24).
 #pragma once
 
+#include "frg_control.cuh"
 #include "frg_device.cuh"
 
 namespace frg {
@@ -316,6 +317,37 @@ template <int NP, int FLUX, int AV>
 __global__ void __launch_bounds__(256)
     stage1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const StageBufs B) {
   stage1d_tile<NP, FLUX, AV>(ops, M, P, B, blockIdx.x * Tile1D<NP>::TX);
+}
+
+// All threads of the cluster: prior global and shared writes of every CTA
+// become visible to every CTA of the cluster (release / acquire).
+FRG_DEV void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;\n" ::: "memory");
+}
+
+// Small 1D solves: one thread-block cluster covers the whole mesh, one tile
+// per CTA, and runs `nsteps` passes of the ssp_rk3!/ssp_rk2! loop body (the
+// top, the stages, the bottom) with cluster barriers between them, instead of
+// five kernel launches per step.  Every CTA runs the same tile function on the
+// same tile as stage1d_kernel, so the steps are those of the launched path bit
+// for bit.  The CTAs take the same barriers in the same order; a tile whose
+// step is inactive returns from the tile function, not from the kernel.
+template <int NP, int FLUX, int AV>
+__global__ void __launch_bounds__(256)
+    loop1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const Loop1DBufs L, DevScalars* sc,
+                  int nsteps) {
+  const int x0 = blockIdx.x * Tile1D<NP>::TX;
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  for (int n = 0; n < nsteps; ++n) {
+    if (lead) step_begin_device(sc);
+    cluster_barrier();
+    for (int s = 0; s < L.nstages; ++s) {
+      stage1d_tile<NP, FLUX, AV>(ops, M, P, L.st[s], x0);
+      cluster_barrier();
+    }
+    if (lead) step_end_device(sc, L.nstages);
+    cluster_barrier();
+  }
 }
 
 }  // namespace frg
