@@ -338,14 +338,18 @@ __global__ void __launch_bounds__(256)
                   int nsteps) {
   const int x0 = blockIdx.x * Tile1D<NP>::TX;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  if (lead) step_begin_device(sc);
+  cluster_barrier();
   for (int n = 0; n < nsteps; ++n) {
-    if (lead) step_begin_device(sc);
-    cluster_barrier();
     for (int s = 0; s < L.nstages; ++s) {
       stage1d_tile<NP, FLUX, AV>(ops, M, P, L.st[s], x0);
       cluster_barrier();
     }
-    if (lead) step_end_device(sc, L.nstages);
+    // the bottom of this pass and the top of the next, by the same thread
+    if (lead) {
+      step_end_device(sc, L.nstages);
+      if (n + 1 < nsteps) step_begin_device(sc);
+    }
     cluster_barrier();
   }
 }
