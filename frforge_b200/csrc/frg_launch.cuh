@@ -154,10 +154,11 @@ int launch1d_inst(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
 }
 
 // nsteps steps of a 1D solve of at most kLoop1DMaxTiles tiles by one cluster
-template <int NP, int FLUX, int AV>
-int loop1d_inst(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
-  using S = Smem1D<NP>;
-  auto kern = loop1d_kernel<NP, FLUX, AV>;
+// of LTX-element tiles
+template <int NP, int FLUX, int AV, int LTX>
+int loop1d_tx(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+  using S = Smem1D<NP, LTX>;
+  auto kern = loop1d_kernel<NP, FLUX, AV, LTX>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
@@ -179,6 +180,14 @@ int loop1d_inst(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nst
   cfg.attrs = at;
   cfg.numAttrs = 1;
   return (int)cudaLaunchKernelEx(&cfg, kern, make_ops<NP>(*L.ops), L.mesh, L.phys, lb, sc, nsteps);
+}
+// half-width tiles where the mesh fits the cluster with them: more CTAs,
+// fewer passes per thread in the staging and epilogue loops
+template <int NP, int FLUX, int AV>
+int loop1d_inst(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+  constexpr int TXH = Tile1D<NP>::TX / 2;
+  if (L.mesh.nel <= kLoop1DMaxTiles * TXH) return loop1d_tx<NP, FLUX, AV, TXH>(L, lb, sc, nsteps, st);
+  return loop1d_tx<NP, FLUX, AV, Tile1D<NP>::TX>(L, lb, sc, nsteps, st);
 }
 
 template <int NP>

@@ -19,9 +19,9 @@ struct Tile1D {
   static constexpr int TX = 64;
 };
 
-template <int NP>
+template <int NP, int TXV = Tile1D<NP>::TX>
 struct Smem1D {
-  static constexpr int NEQ = 3, TX = Tile1D<NP>::TX, NSLOT = TX + 2;
+  static constexpr int NEQ = 3, TX = TXV, NSLOT = TX + 2;
   static constexpr int oU = 0;
   static constexpr int oF = oU + NSLOT * NEQ * NP;
   static constexpr int oG = oF + TX * NEQ * NP;
@@ -33,11 +33,11 @@ struct Smem1D {
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
 };
 
-// One tile of one stage; x0: first element of the tile.
-template <int NP, int FLUX, int AV>
+// One tile of one stage; x0: first element of the tile; TXV elements per tile.
+template <int NP, int FLUX, int AV, int TXV = Tile1D<NP>::TX>
 __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev& M, const Phys& P,
                                              const StageBufs& B, const int x0) {
-  using S = Smem1D<NP>;
+  using S = Smem1D<NP, TXV>;
   constexpr int NEQ = 3, TX = S::TX, NSLOT = S::NSLOT;
   constexpr bool kBR0 = (AV == kAvBR0);
   constexpr bool kAV = (AV != kAvNone);
@@ -326,23 +326,23 @@ FRG_DEV void cluster_barrier() {
 }
 
 // Small 1D solves: one thread-block cluster covers the whole mesh, one tile
-// per CTA, and runs `nsteps` passes of the ssp_rk3!/ssp_rk2! loop body (the
+// of LTX elements per CTA, and runs `nsteps` passes of the ssp_rk3!/ssp_rk2! loop body (the
 // top, the stages, the bottom) with cluster barriers between them, instead of
 // five kernel launches per step.  Every CTA runs the same tile function on the
 // same tile as stage1d_kernel, so the steps are those of the launched path bit
 // for bit.  The CTAs take the same barriers in the same order; a tile whose
 // step is inactive returns from the tile function, not from the kernel.
-template <int NP, int FLUX, int AV>
+template <int NP, int FLUX, int AV, int LTX>
 __global__ void __launch_bounds__(256)
     loop1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const Loop1DBufs L, DevScalars* sc,
                   int nsteps) {
-  const int x0 = blockIdx.x * Tile1D<NP>::TX;
+  const int x0 = blockIdx.x * LTX;
   const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
   if (lead) step_begin_device(sc);
   cluster_barrier();
   for (int n = 0; n < nsteps; ++n) {
     for (int s = 0; s < L.nstages; ++s) {
-      stage1d_tile<NP, FLUX, AV>(ops, M, P, L.st[s], x0);
+      stage1d_tile<NP, FLUX, AV, LTX>(ops, M, P, L.st[s], x0);
       cluster_barrier();
     }
     // the bottom of this pass and the top of the next, by the same thread
