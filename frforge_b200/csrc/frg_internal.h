@@ -209,6 +209,9 @@ struct Loop1DBufs {
 // Largest 1D mesh, in tiles, that one thread-block cluster steps by itself
 // (one tile per CTA; 8 is the portable cluster size).
 constexpr int kLoop1DMaxTiles = 8;
+// Largest cluster of the narrowest 1D loop tiles (a non-portable size, used
+// only where the device can schedule it).
+constexpr int kLoop1DMaxCluster = 16;
 // Returns 0 or a CUDA error code.
 int launch_stage2d(const Launch2D& L, const StageBufs& b, void* stream);
 // batched stage launch over a group's tile list (same NP, flux, AV, tables)

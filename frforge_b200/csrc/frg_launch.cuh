@@ -156,17 +156,20 @@ int launch1d_inst(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
 // nsteps steps of a 1D solve of at most kLoop1DMaxTiles tiles by one cluster
 // of LTX-element tiles
 template <int NP, int FLUX, int AV, int LTX>
-int loop1d_tx(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
+int loop1d_tx(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st,
+              int max_cluster = kLoop1DMaxTiles) {
   using S = Smem1D<NP, LTX>;
   auto kern = loop1d_kernel<NP, FLUX, AV, LTX>;
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+    if (e == cudaSuccess && max_cluster > kLoop1DMaxTiles)
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return (int)e;
     configured = true;
   }
   const int ntiles = (L.mesh.nel + S::TX - 1) / S::TX;
-  if (ntiles < 1 || ntiles > kLoop1DMaxTiles) return (int)cudaErrorInvalidValue;
+  if (ntiles < 1 || ntiles > max_cluster) return (int)cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(ntiles);
   cfg.blockDim = dim3(256);
@@ -181,11 +184,47 @@ int loop1d_tx(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nstep
   cfg.numAttrs = 1;
   return (int)cudaLaunchKernelEx(&cfg, kern, make_ops<NP>(*L.ops), L.mesh, L.phys, lb, sc, nsteps);
 }
-// half-width tiles where the mesh fits the cluster with them: more CTAs,
-// fewer passes per thread in the staging and epilogue loops
+// Whether a cluster of n CTAs of this loop kernel can be scheduled (n > 8
+// is a non-portable size, allowed on this kernel first).
+template <int NP, int FLUX, int AV, int LTX>
+bool loop1d_cluster_fits(int n) {
+  using S = Smem1D<NP, LTX>;
+  auto kern = loop1d_kernel<NP, FLUX, AV, LTX>;
+  static int fits = -1;  // per instantiation; n is the same kLoop1DMaxCluster every call
+  if (fits < 0) {
+    fits = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes) == cudaSuccess &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(n);
+      cfg.blockDim = dim3(256);
+      cfg.dynamicSmemBytes = S::bytes;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = n;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, kern, &cfg) == cudaSuccess && nc >= 1) fits = 1;
+    }
+    cudaGetLastError();  // a refused query leaves no sticky error
+  }
+  return fits == 1;
+}
+
+// The narrowest tiles whose cluster holds the mesh: quarter-width tiles on up
+// to kLoop1DMaxCluster CTAs where such a cluster can be scheduled, else
+// half-width tiles on up to 8, else full tiles.  Narrower tiles mean more
+// CTAs and fewer passes per thread in each phase.
 template <int NP, int FLUX, int AV>
 int loop1d_inst(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nsteps, cudaStream_t st) {
-  constexpr int TXH = Tile1D<NP>::TX / 2;
+  constexpr int TXQ = Tile1D<NP>::TX / 4, TXH = Tile1D<NP>::TX / 2;
+  const int nq = (L.mesh.nel + TXQ - 1) / TXQ;
+  if (nq <= kLoop1DMaxTiles ||
+      (nq <= kLoop1DMaxCluster && loop1d_cluster_fits<NP, FLUX, AV, TXQ>(kLoop1DMaxCluster)))
+    return loop1d_tx<NP, FLUX, AV, TXQ>(L, lb, sc, nsteps, st, kLoop1DMaxCluster);
   if (L.mesh.nel <= kLoop1DMaxTiles * TXH) return loop1d_tx<NP, FLUX, AV, TXH>(L, lb, sc, nsteps, st);
   return loop1d_tx<NP, FLUX, AV, Tile1D<NP>::TX>(L, lb, sc, nsteps, st);
 }
