@@ -521,6 +521,12 @@ void release(frg_solve* s) {
 
 }  // namespace
 
+namespace frg {
+namespace rt {
+int validate_desc(frg_ctx* c, const frg_solve_desc* d) { return validate(c, d); }
+}  // namespace rt
+}  // namespace frg
+
 extern "C" {
 
 int frg_abi_version(void) { return FRG_ABI_VERSION; }
@@ -778,8 +784,8 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
     batch_tile_shape(1, s->np, 0, &tx, &ty);
     loop1d = (s->nel + tx - 1) / tx <= kLoop1DMaxTiles;
   }
-  if (use_graph && !loop1d) {
-    // the graph depends only on buffers, tables and the dt mode of the solve
+  // the graph depends only on buffers, tables and the dt mode of the solve
+  auto ensure_graph = [&]() -> int {
     if (!s->graph || s->graph_steps != K || s->graph_lambda != want_lambda) {
       if (s->graph) {
         cudaGraphExecDestroy(s->graph);
@@ -798,7 +804,9 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
       s->graph_steps = K;
       s->graph_lambda = want_lambda;
     }
-  }
+    return FRG_OK;
+  };
+  if (use_graph && !loop1d && (rc = ensure_graph())) return rc;
   cudaEvent_t ev[6];
   double acc[3] = {0.0, 0.0, 0.0};
   int64_t nt = 0;
@@ -810,7 +818,14 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
       lb.nstages = s->time_scheme == FRG_TIME_SSP_RK2 ? 2 : 3;
       for (int k = 0; k < lb.nstages; ++k) lb.st[k] = stage_bufs(s, k + 1, want_lambda);
       const int e = launch_loop1d(s->L1, lb, s->sc, K, s->ctx->stream);
-      if (e) return cuda_err(s->ctx, (cudaError_t)e, "1D loop kernel launch");
+      if (e) {
+        // a cluster the device refuses at launch ran nothing: step the solve
+        // with step graphs instead
+        cudaGetLastError();
+        loop1d = false;
+        if ((rc = ensure_graph())) return rc;
+        continue;
+      }
     } else if (use_graph) {
       FRG_CUDA(cudaGraphLaunch(s->graph, s->ctx->stream), "graph launch");
     } else {

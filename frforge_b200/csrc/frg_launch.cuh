@@ -5,11 +5,37 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "frg_batch.cuh"
 #include "frg_stage1d.cuh"
 #include "frg_stage2d.cuh"
 
 namespace frg {
+
+// Kernel attributes (dynamic shared memory size, cluster size) belong to a
+// function on one device.  KernelSetup records, per device, that a kernel's
+// attributes were set, so a process whose contexts live on several GPUs sets
+// them on each, and host threads that launch at the same time set them once.
+constexpr int kMaxDevices = 64;
+struct KernelSetup {
+  std::mutex mu;
+  std::atomic<bool> done[kMaxDevices] = {};
+  // Runs set() once per device (again after a failure); returns 0 or a CUDA
+  // error code.
+  template <class F>
+  int ensure(F&& set) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return (int)cudaErrorInvalidDevice;
+    if (done[dev].load(std::memory_order_acquire)) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev].load(std::memory_order_relaxed)) return 0;
+    const int rc = set();
+    if (rc == 0) done[dev].store(true, std::memory_order_release);
+    return rc;
+  }
+};
 
 template <int NP>
 OpsT<NP> make_ops(const HostOps& h) {
@@ -100,13 +126,13 @@ int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
   // affine and curved meshes have kernels of their own
   auto kaff = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT, 0>;
   auto kcur = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT, 1>;
-  static bool configured = false;  // the attribute belongs to the functions
-  if (!configured) {
+  static KernelSetup setup;
+  const int se = setup.ensure([&] {
     cudaError_t e = cudaFuncSetAttribute(kaff, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kcur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
-    if (e != cudaSuccess) return (int)e;
-    configured = true;
-  }
+    return (int)e;
+  });
+  if (se) return se;
   auto kern = L.mesh.curved ? kcur : kaff;
   dim3 grid((L.mesh.nx + VV::TX - 1) / VV::TX, (L.mesh.ny + VV::TY - 1) / VV::TY);
   kern<<<grid, VV::NT, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
@@ -142,12 +168,10 @@ template <int NP, int FLUX, int AV>
 int launch1d_inst(const Launch1D& L, const StageBufs& b, cudaStream_t st) {
   using S = Smem1D<NP>;
   auto kern = stage1d_kernel<NP, FLUX, AV>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
-    if (e != cudaSuccess) return (int)e;
-    configured = true;
-  }
+  static KernelSetup setup;
+  const int se = setup.ensure(
+      [&] { return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes); });
+  if (se) return se;
   dim3 grid((L.mesh.nel + S::TX - 1) / S::TX);
   kern<<<grid, 256, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
   return (int)cudaGetLastError();
@@ -160,14 +184,15 @@ int loop1d_tx(const Launch1D& L, const Loop1DBufs& lb, DevScalars* sc, int nstep
               int max_cluster = kLoop1DMaxTiles) {
   using S = Smem1D<NP, LTX>;
   auto kern = loop1d_kernel<NP, FLUX, AV, LTX>;
-  static bool configured = false;
-  if (!configured) {
+  // every instantiation launches with a single max_cluster value
+  static KernelSetup setup;
+  const int se = setup.ensure([&] {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
     if (e == cudaSuccess && max_cluster > kLoop1DMaxTiles)
       e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return (int)e;
-    configured = true;
-  }
+    return (int)e;
+  });
+  if (se) return se;
   const int ntiles = (L.mesh.nel + S::TX - 1) / S::TX;
   if (ntiles < 1 || ntiles > max_cluster) return (int)cudaErrorInvalidValue;
   cudaLaunchConfig_t cfg = {};
@@ -190,9 +215,14 @@ template <int NP, int FLUX, int AV, int LTX>
 bool loop1d_cluster_fits(int n) {
   using S = Smem1D<NP, LTX>;
   auto kern = loop1d_kernel<NP, FLUX, AV, LTX>;
-  static int fits = -1;  // per instantiation; n is the same kLoop1DMaxCluster every call
-  if (fits < 0) {
-    fits = 0;
+  // per device: 0 unknown, 1 fits, 2 does not (n is the same
+  // kLoop1DMaxCluster every call)
+  static std::atomic<int> fits[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+  int f = fits[dev].load(std::memory_order_acquire);
+  if (f == 0) {
+    f = 2;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes) == cudaSuccess &&
         cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
       cudaLaunchConfig_t cfg = {};
@@ -207,11 +237,12 @@ bool loop1d_cluster_fits(int n) {
       cfg.attrs = at;
       cfg.numAttrs = 1;
       int nc = 0;
-      if (cudaOccupancyMaxActiveClusters(&nc, kern, &cfg) == cudaSuccess && nc >= 1) fits = 1;
+      if (cudaOccupancyMaxActiveClusters(&nc, kern, &cfg) == cudaSuccess && nc >= 1) f = 1;
     }
     cudaGetLastError();  // a refused query leaves no sticky error
+    fits[dev].store(f, std::memory_order_release);
   }
-  return fits == 1;
+  return f == 1;
 }
 
 // The narrowest tiles whose cluster holds the mesh: quarter-width tiles on up
@@ -283,12 +314,10 @@ int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles
   using VV = typename Variants2D<NP>::template V_<V>;
   using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB, VV::NT>;
   auto kern = stage2d_batch_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
-    if (e != cudaSuccess) return (int)e;
-    configured = true;
-  }
+  static KernelSetup setup;
+  const int se = setup.ensure(
+      [&] { return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes); });
+  if (se) return se;
   if (ntiles > 0) kern<<<ntiles, VV::NT, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
   return (int)cudaGetLastError();
 }
@@ -321,12 +350,10 @@ int batch1d_inst(const HostOps& h, const BatchInst* insts, const BatchTile* tile
                  int mode, cudaStream_t st) {
   using S = Smem1D<NP>;
   auto kern = stage1d_batch_kernel<NP, FLUX, AV>;
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
-    if (e != cudaSuccess) return (int)e;
-    configured = true;
-  }
+  static KernelSetup setup;
+  const int se = setup.ensure(
+      [&] { return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes); });
+  if (se) return se;
   if (ntiles > 0) kern<<<ntiles, 256, S::bytes, st>>>(make_ops<NP>(h), insts, tiles, stage, mode);
   return (int)cudaGetLastError();
 }

@@ -30,7 +30,7 @@
 #include <cstring>
 #include <mutex>
 
-#include "frg_internal.h"
+#include "frg_runtime.h"
 
 namespace frg {
 
@@ -51,14 +51,29 @@ namespace {
 std::mutex g_na_mu;
 double* g_na_ptr[64] = {nullptr};  // device address of the scratch array, per device
 
-// Host staging for the mesh arrays (no allocation at call time).
+// Host staging for the row and column arrays (no allocation at call time).
 struct NaHost {
   double cols[3 * kNaMaxSide];
   double rows[3 * kNaMaxSide];
-  double hchar[kNaMaxEl];
   double xv[kNaMaxSide + 1], yv[kNaMaxSide + 1];
 };
 NaHost g_na_host;
+
+// Element sizes h_char = min(dx, dy) (Mesh2D.jl:35-91) from the column and
+// row half-widths (2 Jx = dx exactly), and the status block of one residual
+// evaluation: O(nel) work on the device instead of a host loop and copy.
+__global__ void noalloc_setup_kernel(int nx, int ny, const double* Jx, const double* Jy, double* hchar,
+                                     DevScalars* sc, double t, int two_p1) {
+  const int nel = nx * ny;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += gridDim.x * blockDim.x)
+    hchar[e] = fmin(2.0 * Jx[e % nx], 2.0 * Jy[e / nx]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    DevScalars z = {};
+    z.t = t;
+    z.two_p1 = two_p1;
+    *sc = z;
+  }
+}
 
 }  // namespace
 }  // namespace frg
@@ -68,17 +83,13 @@ using namespace frg;
 extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, double* du, double t,
                                       void* stream) {
   if (!d || !u || !du) return FRG_ERR_INVALID_ARG;
-  if (d->dim != 2 || d->p < 1 || d->p > FRG_MAX_NP - 1) return FRG_ERR_INVALID_ARG;
-  if (d->nx < 1 || d->ny < 1 || d->nx > kNaMaxSide || d->ny > kNaMaxSide ||
-      (long long)d->nx * d->ny > kNaMaxEl)
+  // the checks of frg_solve_create, then the limits of this entry point
+  const int vrc = rt::validate_desc(nullptr, d);
+  if (vrc) return vrc;
+  if (d->dim != 2) return FRG_ERR_INVALID_ARG;
+  if (d->nx > kNaMaxSide || d->ny > kNaMaxSide || (long long)d->nx * d->ny > kNaMaxEl)
     return FRG_ERR_INVALID_ARG;  // beyond the fixed scratch size
   if (d->geometry != FRG_GEOM_AFFINE || d->solid) return FRG_ERR_INVALID_ARG;
-  if (d->method != FRG_METHOD_NULL && d->method != FRG_METHOD_PERSSON) return FRG_ERR_UNSUPPORTED_HOOK;
-  if ((d->bc[0].kind == FRG_BC_PERIODIC) != (d->bc[1].kind == FRG_BC_PERIODIC) ||
-      (d->bc[2].kind == FRG_BC_PERIODIC) != (d->bc[3].kind == FRG_BC_PERIODIC))
-    return FRG_ERR_INVALID_ARG;
-  if (!d->x_vertices && !(d->x_right > d->x_left)) return FRG_ERR_INVALID_ARG;
-  if (!d->y_vertices && !(d->y_top > d->y_bottom)) return FRG_ERR_INVALID_ARG;
 
   std::lock_guard<std::mutex> lock(g_na_mu);
   int dev = 0;
@@ -106,31 +117,30 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
     std::memcpy(h.yv, d->y_vertices, sizeof(double) * (ny + 1));
   else
     julia_linspace(d->y_bottom, d->y_top, ny + 1, h.yv);
+  // xc, Jx, 1/Jx packed at stride nx (yc, Jy, 1/Jy at stride ny), so one
+  // copy of 3 nx (3 ny) doubles moves what the mesh uses
   for (int i = 0; i < nx; ++i) {
     h.cols[i] = (h.xv[i] + h.xv[i + 1]) / 2.0;
-    h.cols[kNaMaxSide + i] = (h.xv[i + 1] - h.xv[i]) / 2.0;
-    h.cols[2 * kNaMaxSide + i] = 1.0 / h.cols[kNaMaxSide + i];
+    h.cols[nx + i] = (h.xv[i + 1] - h.xv[i]) / 2.0;
+    h.cols[2 * nx + i] = 1.0 / h.cols[nx + i];
   }
   for (int i = 0; i < ny; ++i) {
     h.rows[i] = (h.yv[i] + h.yv[i + 1]) / 2.0;
-    h.rows[kNaMaxSide + i] = (h.yv[i + 1] - h.yv[i]) / 2.0;
-    h.rows[2 * kNaMaxSide + i] = 1.0 / h.rows[kNaMaxSide + i];
+    h.rows[ny + i] = (h.yv[i + 1] - h.yv[i]) / 2.0;
+    h.rows[2 * ny + i] = 1.0 / h.rows[ny + i];
   }
-  for (int e = 0; e < nel; ++e)
-    h.hchar[e] = std::fmin(h.xv[e % nx + 1] - h.xv[e % nx], h.yv[e / nx + 1] - h.yv[e / nx]);
-  DevScalars sc;
-  std::memset(&sc, 0, sizeof(sc));
-  sc.t = t;
-  sc.two_p1 = 2 * d->p + 1;
-
-  cudaError_t e = cudaMemcpyAsync(base + kNaCols, h.cols, sizeof(h.cols), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kNaRows, h.rows, sizeof(h.rows), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kNaHchar, h.hchar, sizeof(double) * nel, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(base + kNaScalars, &sc, sizeof(sc), cudaMemcpyHostToDevice, st);
+  double* cols = base + kNaCols;
+  double* rows = base + kNaRows;
+  DevScalars* dsc = reinterpret_cast<DevScalars*>(base + kNaScalars);
+  cudaError_t e = cudaMemcpyAsync(cols, h.cols, sizeof(double) * 3 * nx, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rows, h.rows, sizeof(double) * 3 * ny, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return FRG_ERR_CUDA;
+  {
+    const int blocks = (nel + 255) / 256 < 1184 ? (nel + 255) / 256 : 1184;
+    noalloc_setup_kernel<<<blocks, 256, 0, st>>>(nx, ny, cols + nx, rows + ny, base + kNaHchar, dsc, t,
+                                                  2 * d->p + 1);
+    if (cudaGetLastError() != cudaSuccess) return FRG_ERR_CUDA;
+  }
 
   Launch2D L{};
   L.ops = &ops;
@@ -140,12 +150,12 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
   M.nel = nel;
   M.px = d->bc[0].kind == FRG_BC_PERIODIC;
   M.py = d->bc[2].kind == FRG_BC_PERIODIC;
-  M.xc = base + kNaCols;
-  M.Jx = base + kNaCols + kNaMaxSide;
-  M.rJx = base + kNaCols + 2 * kNaMaxSide;
-  M.yc = base + kNaRows;
-  M.Jy = base + kNaRows + kNaMaxSide;
-  M.rJy = base + kNaRows + 2 * kNaMaxSide;
+  M.xc = cols;
+  M.Jx = cols + nx;
+  M.rJx = cols + 2 * nx;
+  M.yc = rows;
+  M.Jy = rows + ny;
+  M.rJy = rows + 2 * ny;
   M.hchar = base + kNaHchar;
   for (int k = 0; k < 4; ++k) {
     const frg_bc& b = d->bc[k];
@@ -174,7 +184,6 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
   L.av = d->method == FRG_METHOD_PERSSON ? (d->av_form == FRG_AV_LOCAL_DD ? kAvDD : kAvBR0) : kAvNone;
   L.variant = 0;
 
-  DevScalars* dsc = reinterpret_cast<DevScalars*>(base + kNaScalars);
   double* eps = base + kNaEps;
   if (L.av != kAvNone) {
     // element viscosity of the state (every element is written)

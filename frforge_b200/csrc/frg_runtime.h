@@ -53,6 +53,8 @@ struct frg_solve {
 namespace frg {
 namespace rt {
 int set_err(frg_ctx* c, int code, const std::string& msg);
+// the descriptor checks of frg_solve_create (c may be null)
+int validate_desc(frg_ctx* c, const frg_solve_desc* d);
 int cuda_err(frg_ctx* c, cudaError_t e, const char* what);
 int push_scalars(frg_solve* s);
 int pull_scalars(frg_solve* s);

@@ -34,7 +34,11 @@ struct Smem1D {
 };
 
 // One tile of one stage; x0: first element of the tile; TXV elements per tile.
-template <int NP, int FLUX, int AV, int TXV = Tile1D<NP>::TX>
+// COHERENT: the stage input was written earlier in the same launch by other
+// CTAs (the cluster loop kernel), so it is read through L2 (ld.global.cg)
+// instead of the non-coherent read-only path, which lies outside the memory
+// model's ordering by the cluster barriers.
+template <int NP, int FLUX, int AV, int TXV = Tile1D<NP>::TX, bool COHERENT = false>
 __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev& M, const Phys& P,
                                              const StageBufs& B, const int x0) {
   using S = Smem1D<NP, TXV>;
@@ -97,7 +101,10 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
     const int r = idx % (NSLOT * NP), c = idx / (NSLOT * NP);
     const int s = r / NP, k = r % NP;
     const int el = sEl[s];
-    if (el >= 0) sU[(s * NEQ + c) * NP + k] = __ldg(&B.us[c * cs + (size_t)el * NP + k]);
+    if (el >= 0) {
+      const double* src = &B.us[c * cs + (size_t)el * NP + k];
+      sU[(s * NEQ + c) * NP + k] = COHERENT ? __ldcg(src) : __ldg(src);
+    }
   }
   __syncthreads();
 
@@ -329,9 +336,12 @@ FRG_DEV void cluster_barrier() {
 // of LTX elements per CTA, and runs `nsteps` passes of the ssp_rk3!/ssp_rk2! loop body (the
 // top, the stages, the bottom) with cluster barriers between them, instead of
 // five kernel launches per step.  Every CTA runs the same tile function on the
-// same tile as stage1d_kernel, so the steps are those of the launched path bit
-// for bit.  The CTAs take the same barriers in the same order; a tile whose
-// step is inactive returns from the tile function, not from the kernel.
+// same tile as stage1d_kernel, reading its stage input through L2.  The
+// compiler fuses a few multiply-adds differently when the tile function is
+// inlined here, so the steps agree with the launched path to a few ulps of
+// the state (not bit for bit), with the same step count, time and status.
+// The CTAs take the same barriers in the same order; a tile whose step is
+// inactive returns from the tile function, not from the kernel.
 template <int NP, int FLUX, int AV, int LTX>
 __global__ void __launch_bounds__(256)
     loop1d_kernel(const OpsT<NP> ops, const Mesh1Dev M, const Phys P, const Loop1DBufs L, DevScalars* sc,
@@ -342,7 +352,7 @@ __global__ void __launch_bounds__(256)
   cluster_barrier();
   for (int n = 0; n < nsteps; ++n) {
     for (int s = 0; s < L.nstages; ++s) {
-      stage1d_tile<NP, FLUX, AV, LTX>(ops, M, P, L.st[s], x0);
+      stage1d_tile<NP, FLUX, AV, LTX, true>(ops, M, P, L.st[s], x0);
       cluster_barrier();
     }
     // the bottom of this pass and the top of the next, by the same thread

@@ -44,7 +44,8 @@ typedef enum {
   FRG_ERR_UNSUPPORTED_HOOK = -2, /* a capturing hook with no GPU implementation */
   FRG_ERR_OOM = -3,              /* device allocation / admission budget */
   FRG_ERR_CUDA = -4,             /* CUDA runtime failure; see frg_last_error */
-  FRG_ERR_TIMEOUT = -5,          /* bounded device wait gave up */
+  FRG_ERR_TIMEOUT = -5,          /* reserved: no entry point waits on the device
+                                    with a bound today, so none returns it */
   FRG_ERR_STATE = -6             /* call order (e.g. no state uploaded) */
 } frg_status;
 
@@ -244,8 +245,14 @@ int frg_time_stages(frg_solve* s, int64_t nsteps, double cfl, double fixed_dt,
    invent/confirm loop (src/invent/Robustness.jl:245, src/invent/Confirm.jl:35)
    -- call integrate! (src/time/Integrate.jl:9) once per case, one after the
    other).  Every instance is an ordinary solve with its own state, mesh,
-   tables, dt, time and status; its results are bit-identical to the same
-   solve advanced alone with frg_advance.  Each stage launches one kernel per
+   tables, dt, time and status.  An instance's results do not depend on the
+   mix: they are bit-identical to the same instance alone in a batch.  Against
+   the same solve advanced alone with frg_advance they agree to rounding
+   (the batched kernels read their descriptors from shared memory and the
+   compiler fuses a few multiply-adds differently): within 1e-10 relative,
+   with identical status and step counts.  An instance large enough to run
+   through the single-solve kernels (a solo group) is bit-identical to
+   frg_advance.  Each stage launches one kernel per
    group of instances that share (dim, P, flux, dissipation form, tables),
    over the ragged list of that group's tiles; K steps are captured in one
    CUDA graph.  Adding or removing instances takes effect at the next

@@ -1,8 +1,11 @@
 """Small 1D solves (at most 8 tiles of 64 elements) advance through
 loop1d_kernel: one thread-block cluster runs K steps of the time loop per
-launch.  Its steps are those of the per-stage launches (frg_time_stages runs
-the same steps one kernel per stage), bit for bit, for every scheme, method
-and size up to the 8-tile limit; a larger mesh keeps the step graphs."""
+launch.  Its steps agree with the per-stage launches (frg_time_stages runs
+the same steps one kernel per stage) to rounding -- the compiler fuses a few
+multiply-adds differently in the two kernels, so the bar is 1e-11 relative
+L-infinity with identical step counts, times and status -- for every scheme,
+method and size up to the cluster limit; a larger mesh keeps the step
+graphs."""
 import numpy as np
 import pytest
 

@@ -4,9 +4,12 @@ frg_residual2d_noalloc serves callers that cannot call cudaMalloc when they
 need a residual (their device memory belongs to their own pool or budget):
 they pass device buffers they already own and the library uses a fixed
 device scratch array instead of allocating.  This test calls it through the
-C ABI with torch-owned device buffers and checks it against frg_residual,
-twice in a row on different states, within the residual tolerance (1e-12
-relative L-infinity).  It sits in its own file collected last.
+C ABI with torch-owned device buffers and checks it twice in a row, on
+different states, against frg_residual within the residual tolerance (1e-12
+relative L-infinity) and against the oracle within the production-path
+tolerance (1e-11: library-built tables and exact affine metrics, as in
+test_gpu_parity.test_residual_2d_affine_path).  It sits in its own file
+collected last.
 """
 import ctypes as C
 
@@ -49,6 +52,9 @@ def test_noalloc_matches_frg_residual(cfg):
         got = _noalloc(solve, u)
         assert np.all(np.isfinite(got))
         assert rel_linf(got, ref) <= 1e-12, rel_linf(got, ref)
+        orc.set_state(u)
+        orc.t = 0.0
+        assert rel_linf(got, orc.residual()) <= 1e-11
 
 
 def test_noalloc_rejects_oversized_mesh():
