@@ -495,6 +495,10 @@ def run_batched(args):
     t_seq, t_bat = float(np.median(seq_ms)), float(np.median(bat_ms))
     dof_stages = sum(3 * d * r["n_steps"] for d, r in zip(ndofs, res_bat))
     ngroups = len({(w.p, w.flux) for w in inst})
+    # the packing bound: every instance's DOF-stages at the single-solve
+    # stage kernel's own rate for its (P, flux) on a mesh that fills the GPU
+    rates = single_solve_rates(F, ctx, sorted({(w.p, w.flux) for w in inst}))
+    t_ideal = 1e3 * sum(3 * d * r["n_steps"] / rates[(w.p, w.flux)] for d, r, w in zip(ndofs, res_bat, inst))
     if rank == 0:
         line = {
             "metric": "batched solves/s (64 mixed 2D solves x 200 SSP-RK3 steps) vs one at a time",
@@ -508,6 +512,13 @@ def run_batched(args):
                        "groups": ngroups, "reps": reps},
             "sequential": {"value": len(inst) / (t_seq * 1e-3), "unit": "solves/s", "ms": t_seq},
             "speedup_vs_sequential": t_seq / t_bat,
+            "ideal_speedup": t_seq / t_ideal,
+            "ideal_ms": t_ideal,
+            "packing_efficiency": t_ideal / t_bat,
+            "single_solve_rates": {f"p{p}_{fl}": r for (p, fl), r in rates.items()},
+            "ideal_note": "ideal_ms = sum over instances of DOF-stages / the single-solve stage kernel's rate for "
+                          "that (P, flux) on a 512^2 (P<=3) or 384^2 (P>=4) periodic mesh, measured in this run: "
+                          "the time of a perfectly packed batch; ideal_speedup = sequential ms / ideal_ms",
             "dof_stage_per_s": dof_stages / (t_bat * 1e-3),
             "statuses": sorted({r["status"] for r in res_bat}),
             "max_rel_linf_vs_sequential": worst,
@@ -522,6 +533,27 @@ def run_batched(args):
     for s in solves:
         s.close()
     return 0
+
+
+def single_solve_rates(F, ctx, keys, steps: int = 6):
+    """DOF-stage/s of the single-solve stage kernels per (P, flux), Persson
+    BR0, on a mesh that fills the GPU (512^2 for P <= 3, 384^2 above): the
+    mean stage-kernel time of `steps` SSP-RK3 steps of a periodic density
+    wave, CUDA events around every stage launch (frg_time_stages)."""
+    from frforge_b200.workloads import Workload2D
+
+    out = {}
+    for p, flux in keys:
+        n = 512 if p <= 3 else 384
+        w = Workload2D("c2", n, p, flux, "persson_av", 0.1, True, 0.1, steps)
+        st, m = w.build(F)
+        s = F.GpuSolve(st, F.Euler2D(1.4), m, ctx=ctx)
+        s.upload(st.u, 0.0)
+        s.autotune(reps=3)
+        stage_ms, _ = s.time_stages(steps, cfl=w.cfl)
+        out[(p, flux)] = s.ndof / (float(np.mean(stage_ms)) * 1e-3)
+        s.close()
+    return out
 
 
 def run_served(args):

@@ -1,13 +1,23 @@
-"""Parity at the benchmark sizes.
+"""Parity at the benchmark sizes and lengths.
 
-* The 512^2 P=3 HLLC + Persson BR0 workload (the bench's case): two SSP-RK3
-  steps on the GPU against the oracle on the same seeded state.
-* The 128^2 P=4 Rusanov + Persson periodic density wave: 100 steps against
-  the oracle, and conservation of every component's discrete mass (periodic
-  domain) measured on the GPU state with the device diagnostics.
+* The 512^2 P=3 HLLC + Persson BR0 workload (the bench's case, seeded
+  four-quadrant IC with jump_scale 0.25):
+  - two SSP-RK3 steps against the oracle on the same state (tight bar);
+  - 100 steps against the oracle: relative L1 <= 1e-8 with identical status,
+    step count, positivity and non-finite flags (the shocked-case bar);
+  - its full 1000 steps against the oracle's recorded summary of the same
+    run (tests/golden/c3_oracle_summary.json, written by
+    tests/golden/make_c3_summary.py): step counts, times, discrete masses,
+    density extrema and flags at steps 100, 250, 500 and 1000, from the
+    device diagnostics.
+* The 128^2 P=4 Rusanov + Persson periodic density wave for its full 500
+  steps against the oracle (smooth-case bar 1e-9), and conservation of every
+  component's discrete mass measured on the GPU state.
 
-The oracle runs with all host threads; each case takes seconds on the host.
+The oracle runs with all host threads; the longest case (100 steps of the
+512^2 workload) takes about half a minute on 16 host threads.
 """
+import json
 import math
 import os
 
@@ -47,16 +57,60 @@ def test_512sq_p3_hllc_two_steps():
     assert np.max(np.abs(u - orc.u)) / np.max(np.abs(orc.u)) <= 1e-10
 
 
-def test_128sq_p4_periodic_100_steps_and_mass():
+def test_512sq_p3_hllc_100_steps():
+    st, m = C3.build(F)
+    orc = _oracle_for(C3)
+    orc.set_state(st.u)
+    r_ref = orc.integrate(1e9, cfl=C3.cfl, max_steps=100)
+    s = F.GpuSolve(st, F.Euler2D(1.4), m)
+    s.upload(st.u, 0.0)
+    r = s.advance(1e9, cfl=C3.cfl, max_steps=100)
+    d = s.diagnostics()
+    u, t = s.download()
+    assert r["status"] == r_ref["status"] == "max_steps" and r["n_steps"] == r_ref["n_steps"] == 100
+    assert t == pytest.approx(orc.t, rel=1e-12)
+    assert _rel_l1(u, orc.u) <= 1e-8
+    assert d["positivity_ok"] == orc.positivity_ok()
+    assert (d["nonfinite"] > 0) == orc.has_nonfinite() == False  # noqa: E712
+
+
+def _c3_summary():
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c3_oracle_summary.json")) as f:
+        return json.load(f)
+
+
+def test_512sq_p3_hllc_1000_steps_against_oracle_summary():
+    ref = _c3_summary()
+    st, m = C3.build(F)
+    s = F.GpuSolve(st, F.Euler2D(1.4), m)
+    s.upload(st.u, 0.0)
+    done = 0
+    for cp in ref["checkpoints"]:
+        r = s.advance(1e9, cfl=C3.cfl, max_steps=cp["n_steps"] - done)
+        done += r["n_steps"]
+        d = s.diagnostics()
+        assert r["status"] == cp["status"] and done == cp["n_steps"], (r, cp)
+        assert d["t"] == pytest.approx(cp["t"], rel=1e-12)
+        for c in range(4):
+            # transmissive boundaries: the masses move with the boundary fluxes
+            assert d["mass"][c] == pytest.approx(cp["mass"][c], rel=1e-10, abs=1e-13), (done, c)
+        assert d["rho_min"] == pytest.approx(cp["rho_min"], rel=1e-8), done
+        assert d["rho_max"] == pytest.approx(cp["rho_max"], rel=1e-8), done
+        assert d["positivity_ok"] == cp["positivity_ok"]
+        assert (d["nonfinite"] > 0) == cp["nonfinite"]
+    assert done == 1000
+
+
+def test_128sq_p4_periodic_500_steps_and_mass():
     st, m = C2.build(F)
     orc = _oracle_for(C2)
     orc.set_state(st.u)
     mass0 = [orc.discrete_mass(c) for c in range(4)]
-    r_ref = orc.integrate(1e9, cfl=C2.cfl, max_steps=100)
+    r_ref = orc.integrate(1e9, cfl=C2.cfl, max_steps=C2.steps)
     s = F.GpuSolve(st, F.Euler2D(1.4), m)
     s.upload(st.u, 0.0)
-    r = s.advance(1e9, cfl=C2.cfl, max_steps=100)
-    assert r["status"] == r_ref["status"] and r["n_steps"] == r_ref["n_steps"] == 100
+    r = s.advance(1e9, cfl=C2.cfl, max_steps=C2.steps)
+    assert r["status"] == r_ref["status"] and r["n_steps"] == r_ref["n_steps"] == C2.steps == 500
     d = s.diagnostics()
     u, t = s.download()
     assert t == pytest.approx(orc.t, rel=1e-12)
