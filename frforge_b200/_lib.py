@@ -166,6 +166,12 @@ SIGNATURES = {
     "frg_get_variant": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "frg_set_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp]),
+    "frg_autotune_table_load": (C.c_int, [C.c_char_p]),
+    "frg_autotune_table_save": (C.c_int, [C.c_char_p]),
+    "frg_autotune_table_set": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "frg_autotune_table_get": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "frg_autotune_table_clear": (C.c_int, []),
+    "frg_autotune_table_size": (C.c_int, []),
     "frg_residual2d_noalloc": (C.c_int, [C.POINTER(frg_solve_desc), C.c_void_p, C.c_void_p,
                                          C.c_double, C.c_void_p]),
     "frg_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
@@ -173,6 +179,7 @@ SIGNATURES = {
     "frg_batch_add": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(C.c_int)]),
     "frg_batch_remove": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_batch_get_solve": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "frg_batch_slot_group": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "frg_batch_set_multirate": (C.c_int, [C.c_void_p, C.c_int]),
     "frg_batch_start": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_int64]),

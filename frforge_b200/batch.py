@@ -63,6 +63,14 @@ class Batch:
         round (results are unchanged; ``run``'s max_steps counts rounds)."""
         self._chk(L.load().frg_batch_set_multirate(self.handle, 1 if on else 0), "frg_batch_set_multirate")
 
+    def group_of(self, slot: int):
+        """(tile variant, solo) of the group the slot ran in at the last run:
+        the autotune table's variant for its key, or -1 for the default tile."""
+        v, s = C.c_int(), C.c_int()
+        self._chk(L.load().frg_batch_slot_group(self.handle, int(slot), C.byref(v), C.byref(s)),
+                  "frg_batch_slot_group")
+        return v.value, bool(s.value)
+
     def _solve(self, slot: int):
         s = C.c_void_p()
         self._chk(L.load().frg_batch_get_solve(self.handle, int(slot), C.byref(s)), "frg_batch_get_solve")

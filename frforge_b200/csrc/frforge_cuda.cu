@@ -623,6 +623,8 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
     s->L2.flux = d->flux;
     s->L2.av = av;
     s->L2.variant = 0;
+    int tv = 0;
+    if (d->dim == 2 && autotune_table_lookup(d->p, d->flux, av, s->L2.mesh.curved ? 1 : 0, &tv)) s->L2.variant = tv;
     s->L1.ops = &s->ops;
     s->L1.phys = P;
     s->L1.flux = d->flux;
@@ -944,6 +946,8 @@ int frg_autotune(frg_solve* s, int reps, int* best, double* ms) {
   if (s->dim == 2) s->L2.variant = saved;
   if (rc) return rc;
   if (best) *best = best_v;
+  if (s->dim == 2)
+    autotune_table_record(s->np - 1, s->L2.flux, s->L2.av, s->L2.mesh.curved ? 1 : 0, best_v, best_ms);
   return frg_set_variant(s, best_v);
 }
 

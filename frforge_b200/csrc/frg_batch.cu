@@ -219,7 +219,10 @@ int rebuild(frg_batch* b) {
     if (!s) continue;
     const int av = s->dim == 2 ? s->L2.av : s->L1.av;
     const int flux = s->dim == 2 ? s->L2.flux : s->L1.flux;
-    const int variant = 0;  // the batched kernels use one fixed tile shape per NP
+    // the key's variant from the autotune table, else the fixed default tile
+    int variant = -1;
+    if (s->dim == 2 && !autotune_table_lookup(s->np - 1, flux, av, s->L2.mesh.curved ? 1 : 0, &variant))
+      variant = -1;
     int tx = 1, ty = 1;
     const int per_sm = batch_tile_shape(s->dim, s->np, variant, &tx, &ty);
     // the choice depends on the instance alone, so its results do not
@@ -531,6 +534,18 @@ int frg_batch_get_solve(frg_batch* b, int i, frg_solve** s) {
   if (!b || i < 0 || i >= b->cap || !s) return FRG_ERR_INVALID_ARG;
   *s = b->slot[i];
   return *s ? FRG_OK : FRG_ERR_INVALID_ARG;
+}
+
+int frg_batch_slot_group(frg_batch* b, int i, int* variant, int* solo) {
+  if (!b || i < 0 || i >= b->cap || !b->slot[i]) return FRG_ERR_INVALID_ARG;
+  for (const auto& g : b->groups)
+    for (int m : g.members)
+      if (m == i) {
+        if (variant) *variant = g.variant;
+        if (solo) *solo = g.solo ? 1 : 0;
+        return FRG_OK;
+      }
+  return FRG_ERR_STATE;  // not grouped yet: no frg_batch_run since it was added
 }
 
 // Configure an instance's run (integrate! arguments) and mark it running.

@@ -224,5 +224,9 @@ int launch_batch1d(const HostOps* ops, int flux, int av, const BatchInst* insts,
 int batch_tile_shape(int dim, int np, int variant, int* tx, int* ty);
 int launch_stage1d(const Launch1D& L, const StageBufs& b, void* stream);
 int stage2d_variants(int np);
+// persisted autotune table (frg_autotune.cpp), keyed by (p, FRG_FLUX_*,
+// kAv*, curved): lookup returns 1 and the variant if present
+int autotune_table_lookup(int p, int flux, int av, int curved, int* variant);
+void autotune_table_record(int p, int flux, int av, int curved, int variant, double ms);
 
 }  // namespace frg

@@ -322,9 +322,29 @@ int batch2d_var(const HostOps& h, const BatchInst* insts, const BatchTile* tiles
   return (int)cudaGetLastError();
 }
 
+// variant: a tile variant of the autotune table, or -1 for the default
+// batched tile (Variants2D<NP>::batch)
 template <int NP, int FLUX, int AV>
-int batch2d_inst(const HostOps& h, int /*variant*/, const BatchInst* insts, const BatchTile* tiles, int ntiles,
+int batch2d_inst(const HostOps& h, int variant, const BatchInst* insts, const BatchTile* tiles, int ntiles,
                  int stage, int mode, cudaStream_t st) {
+  switch (variant) {
+    case 0:
+      return batch2d_var<NP, FLUX, AV, 0>(h, insts, tiles, ntiles, stage, mode, st);
+    case 1:
+      if constexpr (Variants2D<NP>::n > 1) return batch2d_var<NP, FLUX, AV, 1>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    case 2:
+      if constexpr (Variants2D<NP>::n > 2) return batch2d_var<NP, FLUX, AV, 2>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    case 3:
+      if constexpr (Variants2D<NP>::n > 3) return batch2d_var<NP, FLUX, AV, 3>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    case 4:
+      if constexpr (Variants2D<NP>::n > 4) return batch2d_var<NP, FLUX, AV, 4>(h, insts, tiles, ntiles, stage, mode, st);
+      break;
+    default:
+      break;
+  }
   return batch2d_var<NP, FLUX, AV, Variants2D<NP>::batch>(h, insts, tiles, ntiles, stage, mode, st);
 }
 
@@ -375,17 +395,42 @@ int batch1d_np(const HostOps& h, int flux, int av, const BatchInst* insts, const
   }
 }
 
+template <int NP, int V>
+int tile_shape_v(int* tx, int* ty) {
+  using VV = typename Variants2D<NP>::template V_<V>;
+  *tx = VV::TX;
+  *ty = VV::TY;
+  return VV::MINB;
+}
+
+// Tile shape and CTAs per SM of the batched kernel for `variant` (-1 or out
+// of range: the default batched tile).
 template <int NP>
-int tile_shape_np(int dim, int /*variant*/, int* tx, int* ty) {
+int tile_shape_np(int dim, int variant, int* tx, int* ty) {
   if (dim == 1) {
     *tx = Tile1D<NP>::TX;
     *ty = 1;
     return 1;
   }
-  using VB = typename Variants2D<NP>::template V_<Variants2D<NP>::batch>;
-  *tx = VB::TX;
-  *ty = VB::TY;
-  return VB::MINB;
+  switch (variant) {
+    case 0:
+      return tile_shape_v<NP, 0>(tx, ty);
+    case 1:
+      if constexpr (Variants2D<NP>::n > 1) return tile_shape_v<NP, 1>(tx, ty);
+      break;
+    case 2:
+      if constexpr (Variants2D<NP>::n > 2) return tile_shape_v<NP, 2>(tx, ty);
+      break;
+    case 3:
+      if constexpr (Variants2D<NP>::n > 3) return tile_shape_v<NP, 3>(tx, ty);
+      break;
+    case 4:
+      if constexpr (Variants2D<NP>::n > 4) return tile_shape_v<NP, 4>(tx, ty);
+      break;
+    default:
+      break;
+  }
+  return tile_shape_v<NP, Variants2D<NP>::batch>(tx, ty);
 }
 
 template <int NP>

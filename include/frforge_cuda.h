@@ -217,6 +217,22 @@ int frg_get_variant(const frg_solve* s, int* variant, int* n_variants);
 int frg_set_variant(frg_solve* s, int variant);
 int frg_autotune(frg_solve* s, int reps, int* best, double* ms);
 
+/* Persisted autotune table (no reference counterpart): the tile variant of
+   the 2D stage kernels per key (p, flux FRG_FLUX_*, av 0 none / 1 BR0 /
+   2 element-local DD, curved 0 affine / 1 curved geometry), shared by the
+   whole process.  frg_autotune records its choice under the solve's key;
+   frg_solve_create starts a 2D solve from its key's variant; the batched
+   engine runs each group of instances with its key's variant (else a fixed
+   default tile).  save writes the table as JSON, load merges a file written
+   by save (FRG_ERR_INVALID_ARG and nothing merged if the file is malformed or
+   names an unknown variant).  get returns FRG_ERR_STATE for an absent key. */
+int frg_autotune_table_load(const char* path);
+int frg_autotune_table_save(const char* path);
+int frg_autotune_table_set(int p, int flux, int av, int curved, int variant);
+int frg_autotune_table_get(int p, int flux, int av, int curved, int* variant);
+int frg_autotune_table_clear(void);
+int frg_autotune_table_size(void);
+
 /* Allocation-free residual evaluation (no counterpart in the reference).
    Same result as frg_residual for a 2D affine mesh without solid mask, for
    callers that cannot call cudaMalloc when they need a residual -- e.g. a
@@ -275,6 +291,12 @@ int frg_batch_set_multirate(frg_batch* b, int on);
 /* The instance's solve: frg_upload_state / frg_download_state /
    frg_residual work on it while it is not running. */
 int frg_batch_get_solve(frg_batch* b, int slot, frg_solve** s);
+/* The group an instance ran in at the last frg_batch_run (no reference
+   counterpart): *variant is the tile variant of its batched kernels (the
+   autotune table's entry for its key, or -1 for the default tile) and *solo
+   whether it runs alone through the single-solve kernels.  FRG_ERR_STATE
+   before its first run. */
+int frg_batch_slot_group(frg_batch* b, int slot, int* variant, int* solo);
 /* Start an instance's run with integrate!'s arguments (as frg_advance). */
 int frg_batch_start(frg_batch* b, int slot, double t_final, double cfl, double fixed_dt,
                     int64_t max_steps);

@@ -301,3 +301,39 @@ def test_start_without_state_and_bad_slot():
     res = b.run()  # nothing running: returns at once
     assert res[i]["status"] in ("ok", "max_steps") and b.n_running == 0
     b.close()
+
+
+def test_autotune_table_selects_solve_and_group_variants():
+    # a table entry for (P=3, HLLC, BR0, affine) sets the variant of a new
+    # solve and of the batched group that runs such instances; results stay
+    # within the batched bar of the oracle-checked single-solve path
+    from frforge_b200 import autotune as T
+
+    T.clear()
+    try:
+        T.set_variant(3, "hllc", "br0", False, 2)
+        kw = dict(p=3, nx=20, ny=20, flux="hllc", method="persson", bcs=("transmissive",) * 4)
+        orc, state, solve = pair_2d(**kw)
+        assert solve.variant()[0] == 2
+        u0 = four_quadrant_state(orc, jump_scale=0.25)
+        run = dict(t_final=1.0, cfl=0.1, max_steps=20)
+        r_ref, u_ref, t_ref = _run_alone(solve, u0, run)
+        # the same run with the default batched tile
+        T.clear()
+        outs = []
+        for v in (None, 2):
+            if v is not None:
+                T.set_variant(3, "hllc", "br0", False, v)
+            b = Batch(capacity=2)
+            i = b.add(state, F.Euler2D(1.4), F.PerssonAVMethod(c_av=0.1))
+            b.upload(i, u0, 0.0)
+            b.start(i, run["t_final"], cfl=run["cfl"], max_steps=run["max_steps"])
+            res = b.run()
+            assert b.group_of(i) == ((-1 if v is None else v), False)
+            assert res[i]["status"] == r_ref["status"] and res[i]["n_steps"] == r_ref["n_steps"]
+            outs.append(b.download(i)[0])
+            b.close()
+        for u in outs:
+            assert rel_linf(u, u_ref) <= 1e-10
+    finally:
+        T.clear()
