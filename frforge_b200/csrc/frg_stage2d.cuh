@@ -250,9 +250,14 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
 // P1-P6 of one tile whose copies are in tb.  WAIT: cp.async groups that may
 // still be pending when the tile starts.
 // CURV: 0 affine mesh, 1 curved mesh, -1 read from the descriptor.
-template <int NP, int FLUX, int AV, class S, int WAIT, int CURV = -1>
+// INT: an interior tile of an affine mesh (tile_is_interior): every slot
+// holds an element, the tile positions are its own elements, there is no
+// solid element and every face is an interior face, so no slot flag is read
+// and no boundary or wall case is compiled.
+template <int NP, int FLUX, int AV, class S, int WAIT, int CURV = -1, bool INT = false>
 FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P, const StageBufs& B,
                           const TileBuf& tb, double* smem, const StageCtl& ctl) {
+  static_assert(!INT || CURV == 0, "interior tiles are affine");
   const bool curved = CURV < 0 ? (M.curved != 0) : (CURV == 1);
   constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, FS = S::FS;
   constexpr int BX = S::BX, NSLOT = S::NSLOT, NOWN = S::NOWN;
@@ -301,7 +306,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     for (int idx = tid; idx < NOWN * NP2; idx += NT) {
       const int o = idx % NOWN, k = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (!(sFlag[s] & kSlotOwn) || (sFlag[s] & kSlotSolid)) continue;
+      if (!INT && (!(sFlag[s] & kSlotOwn) || (sFlag[s] & kSlotSolid))) continue;
       double U[4], F[4], G[4];
 #pragma unroll
       for (int c = 0; c < NEQ; ++c) U[c] = sU[s * ES + c * NP2 + k];
@@ -346,17 +351,17 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         sA = fy * BX + fx + 1;
         sB = sA + BX;
       }
-      const int flA = sFlag[sA], flB = sFlag[sB];
-      if (!((flA | flB) & kSlotOwn)) continue;
+      const int flA = INT ? kSlotOwn : sFlag[sA], flB = INT ? kSlotOwn : sFlag[sB];
+      if (!INT && !((flA | flB) & kSlotOwn)) continue;
       double* out = (vert ? sFV : sFH) + f * FS + q * 8;
-      const int eA = sEl[sA], eB = sEl[sB];
+      const int eA = INT ? 0 : sEl[sA], eB = INT ? 0 : sEl[sB];
       // the face line inside A (its east/north end) and B (west/south end)
       const int lstride = vert ? 1 : NP;
       const int lbase = vert ? NP * q : q;
       double uA[4], uB[4], gA[4], gB[4];
       // g traces use l^T D, whose entries sum to zero: shifting the line by
       // one of its values removes the cancellation of large terms exactly.
-      if (eA >= 0) {
+      if (INT || eA >= 0) {
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           const double* a = sU + sA * ES + c * NP2 + lbase;
@@ -372,7 +377,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           gA[c] = sg;
         }
       }
-      if (eB >= 0) {
+      if (INT || eB >= 0) {
 #pragma unroll
         for (int c = 0; c < NEQ; ++c) {
           const double* b = sU + sB * ES + c * NP2 + lbase;
@@ -392,7 +397,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       // before the numerical flux
       if (kBR0) {
         double gh[4];
-        if (eA >= 0 && eB >= 0) {
+        if (INT || (eA >= 0 && eB >= 0)) {
           // eps/J of both sides; element widths 2 J (exact)
           const double sa = sEps[sA] * (vert ? sRjx[sA] : sRjy[sA]);
           const double sb = sEps[sB] * (vert ? sRjx[sB] : sRjy[sB]);
@@ -417,7 +422,18 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       // boundary).  One flux evaluation serves every case.
       double fL[4], fR[4], fnx = 0.0, fny = 0.0, fsJ = 0.0;
       bool doflux = false;
-      if (eA >= 0 && eB >= 0) {
+      if (INT) {
+        // interior pair, affine unit normal
+        fnx = vert ? 1.0 : 0.0;
+        fny = vert ? 0.0 : 1.0;
+        fsJ = vert ? sJy[sA] : sJx[sA];
+#pragma unroll
+        for (int c = 0; c < NEQ; ++c) {
+          fL[c] = uA[c];
+          fR[c] = uB[c];
+        }
+        doflux = true;
+      } else if (eA >= 0 && eB >= 0) {
         const bool solA = flA & kSlotSolid, solB = flB & kSlotSolid;
         const bool wrapf = (flA | flB) & kSlotWrap;
         if (wrapf && (solA || solB)) {
@@ -534,7 +550,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
         const int o = e + it * EL5;
         if (e < EL5 && o < NOWN) {
           const int s = (o / TX + 1) * BX + (o % TX) + 1;
-          if (sFlag[s] & kSlotOwn) {
+          if (INT || (sFlag[s] & kSlotOwn)) {
             const size_t g0 = (size_t)sEl[s] * NP2 + k;
 #pragma unroll
             for (int c = 0; c < NEQ; ++c) u0r[it][c] = __ldg(&B.u0[c * cs + g0]);
@@ -550,9 +566,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const int j = t % NP, c = t / NP;
       const int ox = o % TX, oy = o / TX;
       const int s = (oy + 1) * BX + ox + 1;
-      if (!(sFlag[s] & kSlotOwn)) continue;
+      if (!INT && !(sFlag[s] & kSlotOwn)) continue;
       double* Fo = sF + o * ES + c * NP2 + NP * j;
-      if (sFlag[s] & kSlotSolid) {
+      if (!INT && (sFlag[s] & kSlotSolid)) {
 #pragma unroll
         for (int i = 0; i < NP; ++i) Fo[i] = 0.0;
         continue;
@@ -607,9 +623,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const int i = t % NP, c = t / NP;
       const int ox = o % TX, oy = o / TX;
       const int s = (oy + 1) * BX + ox + 1;
-      if (!(sFlag[s] & kSlotOwn)) continue;
+      if (!INT && !(sFlag[s] & kSlotOwn)) continue;
       double* Go = sG + o * ES + c * NP2 + i;
-      if (sFlag[s] & kSlotSolid) {
+      if (!INT && (sFlag[s] & kSlotSolid)) {
 #pragma unroll
         for (int j = 0; j < NP; ++j) Go[NP * j] = 0.0;
         continue;
@@ -670,7 +686,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           const int o = e + it * EL;
           if (o >= NOWN) break;
           const int s = (o / TX + 1) * BX + (o % TX) + 1;
-          if (!(sFlag[s] & kSlotOwn)) continue;
+          if (!INT && !(sFlag[s] & kSlotOwn)) continue;
           const size_t g0 = (size_t)sEl[s] * NP2 + k;
           double unv[NEQ];
 #pragma unroll
@@ -712,7 +728,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     for (int idx = tid; idx < NOWN * NEQ * NP2; idx += NT) {
       const int o = idx % NOWN, r = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (sFlag[s] & kSlotOwn) sF[o * ES + r] = sU[s * ES + r];
+      if (INT || (sFlag[s] & kSlotOwn)) sF[o * ES + r] = sU[s * ES + r];
     }
     __syncthreads();
   }
@@ -727,7 +743,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     for (int idx = tid; prime && idx < NOWN * NP2; idx += NT) {
       const int o = idx % NOWN, k = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (!(sFlag[s] & kSlotOwn)) continue;
+      if (!INT && !(sFlag[s] & kSlotOwn)) continue;
       double U[4];
 #pragma unroll
       for (int c = 0; c < NEQ; ++c) U[c] = sF[o * ES + c * NP2 + k];
@@ -740,7 +756,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       for (int idx = tid; idx < NOWN * NP; idx += NT) {
         const int o = idx % NOWN, j = idx / NOWN;
         const int s = (o / TX + 1) * BX + (o % TX) + 1;
-        if (!(sFlag[s] & kSlotOwn)) continue;
+        if (!INT && !(sFlag[s] & kSlotOwn)) continue;
         const double* rho = sF + o * ES + NP * j;
         double col[NP];
 #pragma unroll
@@ -773,7 +789,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     for (int idx = tid; idx < NOWN * NP; idx += NT) {
       const int o = idx % NOWN, i = idx / NOWN;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (!(sFlag[s] & kSlotOwn)) continue;
+      if (!INT && !(sFlag[s] & kSlotOwn)) continue;
       double row[NP];
 #pragma unroll
       for (int k = 0; k < NP; ++k) row[k] = sX[o * WS + i + NP * k];
@@ -794,7 +810,7 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
     double lcta = 0.0;
     for (int o = tid; o < NOWN; o += NT) {
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
-      if (!(sFlag[s] & kSlotOwn)) continue;
+      if (!INT && !(sFlag[s] & kSlotOwn)) continue;
       const int el = sEl[s];
       double etot = 0.0, ehigh = 0.0, lam = 0.0;
 #pragma unroll
@@ -817,11 +833,11 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       lam = jmax(lam, kEps);
       const double sig = persson_sigma(ehigh, etot + P.eps_floor, P.s0, P.kappa, P.eps_floor);
       if (B.mode == kModeSense) {
-        B.sigma_out[el] = (sFlag[s] & kSlotSolid) ? 0.0 : sig;
+        B.sigma_out[el] = (!INT && (sFlag[s] & kSlotSolid)) ? 0.0 : sig;
         continue;
       }
       double ev = 0.0;
-      if (!(sFlag[s] & kSlotSolid) && sig > 0.0) ev = P.c_av * sig * (sHc[s] * frcp((double)P.pm)) * lam;
+      if ((INT || !(sFlag[s] & kSlotSolid)) && sig > 0.0) ev = P.c_av * sig * (sHc[s] * frcp((double)P.pm)) * lam;
       B.eps_out[el] = ev;
     }
     // the warps that hold elements (NOWN <= NT)
@@ -830,6 +846,18 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       if ((tid & 31) == 0 && B.sc) atomic_max_nonneg(&B.sc->lam_bits, lcta);
     }
   }
+}
+
+// A full tile of an affine mesh without solid elements whose one-element
+// halo ring exists on all four sides (inside the mesh or across a periodic
+// boundary): every face of its elements is an interior face.
+template <int TX, int TY>
+FRG_DEV bool tile_is_interior(const Mesh2Dev& M, const int tx0, const int ty0) {
+  if (M.curved || M.solid) return false;
+  if (tx0 + TX > M.nx || ty0 + TY > M.ny) return false;
+  if (!M.px && (tx0 < 1 || tx0 + TX >= M.nx)) return false;
+  if (!M.py && (ty0 < 1 || ty0 + TY >= M.ny)) return false;
+  return true;
 }
 
 // One tile of one stage (single buffer).  tx0, ty0: first element of the
@@ -846,7 +874,10 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
   tile_slots<S>(M, tb, tx0, ty0, ctl.prime);
   __syncthreads();
   tile_issue<NP, AV, S>(M, B, tb, ctl);
-  tile_compute<NP, FLUX, AV, S, 0, CURV>(ops, M, P, B, tb, smem, ctl);
+  if (CURV != 1 && tile_is_interior<TX, TY>(M, tx0, ty0))
+    tile_compute<NP, FLUX, AV, S, 0, 0, true>(ops, M, P, B, tb, smem, ctl);
+  else
+    tile_compute<NP, FLUX, AV, S, 0, CURV>(ops, M, P, B, tb, smem, ctl);
 }
 
 // Single solve, one tile per CTA: the grid covers the mesh with tiles.
