@@ -118,7 +118,7 @@ def make_ic(kind: str, prim=(), x0: float = 0.5, y0: float = 0.5, amp: float = 0
     return ic
 
 
-HOOK_SLOT = {"post_step": 0}
+HOOK_SLOT = {"post_step": 0, "numerical_flux_method": 1}
 
 
 def device_hooks() -> dict:
@@ -195,6 +195,7 @@ SIGNATURES = {
     "frg_server_set_hook": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, _dp, C.c_int]),
     "frg_server_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(frg_ic), C.c_double,
                                        C.c_double, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]),
+    "frg_vtk_point_data": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, C.c_size_t]),
     "frg_diagnostics_compute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int,
                                           C.POINTER(frg_diagnostics)]),
     "frg_server_create": (C.c_int, [C.c_void_p, C.c_int, C.c_size_t, C.c_int64, C.POINTER(C.c_void_p)]),

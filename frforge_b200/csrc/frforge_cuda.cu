@@ -607,6 +607,7 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
     return set_err(c, rc, "operator tables");
   }
   Phys P;
+  P.flux_alpha = 1.0;
   P.gamma = d->gamma;
   P.g1 = d->gamma - 1.0;
   P.c_av = d->c_av;
@@ -628,6 +629,7 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
     s->L1.ops = &s->ops;
     s->L1.phys = P;
     s->L1.flux = d->flux;
+    s->scheme_flux = d->flux;
     s->L1.av = av;
     for (int k = 0; k < 3 && !rc; ++k) rc = dev_alloc(s, &s->U[k], s->ndof);
     for (int k = 0; k < 3 && !rc; ++k) rc = dev_alloc(s, &s->E[k], (size_t)s->nel);

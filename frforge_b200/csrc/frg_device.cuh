@@ -206,6 +206,101 @@ FRG_DEV void iflux2(double gamma, double g1, const double uL[4], const double uR
     rusanov2(gamma, g1, uL, uR, nx, ny, out);
 }
 
+// The normal fluxes above for the unit normals (1, 0) (X = true) and (0, 1)
+// of the faces of an affine mesh: the same formulas with the zero normal
+// component dropped (for finite states the general forms give these values:
+// every term multiplied by the zero component vanishes and the one
+// multiplied by 1 is unchanged), written in the rotated frame
+// (n = normal velocity index, t = tangential).
+template <bool X>
+FRG_DEV void rusanov2_axis(double gamma, double g1, const double uL[4], const double uR[4], double out[4]) {
+  constexpr int n = X ? 1 : 2, t = X ? 2 : 1;
+  const double rL = jfloor(uL[0], kEps), riL = frcp(rL);
+  const double uLv = uL[1] * riL, vLv = uL[2] * riL;
+  const double pL = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
+  const double rR = jfloor(uR[0], kEps), riR = frcp(rR);
+  const double uRv = uR[1] * riR, vRv = uR[2] * riR;
+  const double pR = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
+  const double unL = X ? uLv : vLv, unR = X ? uRv : vRv;
+  double fL[4], fR[4];
+  fL[0] = uL[n];
+  fL[n] = uL[n] * unL + pL;
+  fL[t] = uL[t] * unL;
+  fL[3] = (uL[3] + pL) * unL;
+  fR[0] = uR[n];
+  fR[n] = uR[n] * unR + pR;
+  fR[t] = uR[t] * unR;
+  fR[3] = (uR[3] + pR) * unR;
+  const double cL = fsqrt(gamma * jfloor(pL, kEps) * riL);
+  const double cR = fsqrt(gamma * jfloor(pR, kEps) * riR);
+  const double lam = jmax(fabs(unL) + cL, fabs(unR) + cR);
+  const double hl = 0.5 * lam;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) out[c] = 0.5 * (fL[c] + fR[c]) - hl * (uR[c] - uL[c]);
+}
+
+template <bool X>
+FRG_DEV void hllc2_axis(double gamma, double g1, const double uL[4], const double uR[4], double out[4]) {
+  constexpr int n = X ? 1 : 2, t = X ? 2 : 1;
+  const double rL = jfloor(uL[0], kEps), riL = frcp(rL);
+  const double rR = jfloor(uR[0], kEps), riR = frcp(rR);
+  const double uLv = uL[1] * riL, vLv = uL[2] * riL;
+  const double uRv = uR[1] * riR, vRv = uR[2] * riR;
+  const double pLu = g1 * (uL[3] - 0.5 * rL * (uLv * uLv + vLv * vLv));
+  const double pRu = g1 * (uR[3] - 0.5 * rR * (uRv * uRv + vRv * vRv));
+  const double pL = jfloor(pLu, kEps), pR = jfloor(pRu, kEps);
+  const double unL = X ? uLv : vLv, unR = X ? uRv : vRv;
+  const double cL = fsqrt(gamma * pL * riL), cR = fsqrt(gamma * pR * riR);
+  const double SL = jmin(unL - cL, unR - cR);
+  const double SR = jmax(unL + cL, unR + cR);
+  const double num = pR - pL + rL * unL * (SL - unL) - rR * unR * (SR - unR);
+  const double den = rL * (SL - unL) - rR * (SR - unR);
+  const double SM = fabs(den) < kEps ? 0.5 * (unL + unR) : num * frcp(den);
+  if (0.0 <= SL) {
+    out[0] = uL[n];
+    out[n] = uL[n] * unL + pLu;
+    out[t] = uL[t] * unL;
+    out[3] = (uL[3] + pLu) * unL;
+    return;
+  }
+  if (0.0 >= SR) {
+    out[0] = uR[n];
+    out[n] = uR[n] * unR + pRu;
+    out[t] = uR[t] * unR;
+    out[3] = (uR[3] + pRu) * unR;
+    return;
+  }
+  const bool left = (SL <= 0.0) && (0.0 <= SM);
+  const double* U = left ? uL : uR;
+  const double r = left ? rL : rR, ri = left ? riL : riR;
+  const double un = left ? unL : unR;
+  const double p = left ? pL : pR, pu = left ? pLu : pRu;
+  const double S = left ? SL : SR;
+  double F[4], ust[4];
+  F[0] = U[n];
+  F[n] = U[n] * un + pu;
+  F[t] = U[t] * un;
+  F[3] = (U[3] + pu) * un;
+  ust[n] = SM;                // normal velocity of the star state
+  ust[t] = U[t] * ri;         // tangential velocity, unchanged
+  const double Sun = S - un;
+  const double rB = frcp(S - SM), rA = frcp(r * Sun);
+  const double factor = r * Sun * rB;
+  const double estar = U[3] * ri + (SM - un) * (SM + p * rA);
+  out[0] = F[0] + S * (factor - U[0]);
+  out[n] = F[n] + S * (factor * ust[n] - U[n]);
+  out[t] = F[t] + S * (factor * ust[t] - U[t]);
+  out[3] = F[3] + S * (factor * estar - U[3]);
+}
+
+template <int FLUX, bool X>
+FRG_DEV void iflux2_axis(double gamma, double g1, const double uL[4], const double uR[4], double out[4]) {
+  if (FLUX == FRG_FLUX_HLLC)
+    hllc2_axis<X>(gamma, g1, uL, uR, out);
+  else
+    rusanov2_axis<X>(gamma, g1, uL, uR, out);
+}
+
 // reflect_conserved (2D), BoundaryConditions.jl:43-60
 FRG_DEV void reflect2(const double U[4], double nx, double ny, double out[4]) {
   const double r = jfloor(U[0], kEps), ri = 1.0 / r;
@@ -274,11 +369,14 @@ FRG_DEV double wave_speed1(double gamma, double g1, const double U[3]) {
 }
 
 // rusanov_flux, Rusanov.jl:10-25 with max_wave_speed Euler.jl:107-113
-FRG_DEV void rusanov1(double gamma, double g1, const double uL[3], const double uR[3], double out[3]) {
+// alpha scales the dissipation (a numerical_flux_method override); alpha = 1
+// is the reference's flux exactly.
+FRG_DEV void rusanov1(double gamma, double g1, const double uL[3], const double uR[3], double out[3],
+                      double alpha = 1.0) {
   double fL[3], fR[3];
   flux1(g1, uL, fL);
   flux1(g1, uR, fR);
-  const double lam = jmax(wave_speed1(gamma, g1, uL), wave_speed1(gamma, g1, uR));
+  const double lam = alpha * jmax(wave_speed1(gamma, g1, uL), wave_speed1(gamma, g1, uR));
   const double hl = 0.5 * lam;
 #pragma unroll
   for (int c = 0; c < 3; ++c) out[c] = 0.5 * (fL[c] + fR[c]) - hl * (uR[c] - uL[c]);
@@ -321,11 +419,12 @@ FRG_DEV void hllc1(double gamma, double g1, const double uL[3], const double uR[
 }
 
 template <int FLUX>
-FRG_DEV void iflux1(double gamma, double g1, const double uL[3], const double uR[3], double out[3]) {
+FRG_DEV void iflux1(double gamma, double g1, const double uL[3], const double uR[3], double out[3],
+                    double alpha = 1.0) {
   if (FLUX == FRG_FLUX_HLLC)
     hllc1(gamma, g1, uL, uR, out);
   else
-    rusanov1(gamma, g1, uL, uR, out);
+    rusanov1(gamma, g1, uL, uR, out, alpha);
 }
 
 // 1D exterior state for the domain ends (Residual.jl:63-112): transmissive

@@ -6,6 +6,17 @@
 // implementation per hook slot, chosen with frg_solve_set_hook.
 //
 // Registered implementations:
+//   numerical_flux_method "flux_rusanov"  (1D) the Rusanov flux with its
+//       dissipation scaled by alpha: 1/2 (F(uL) + F(uR)) - 1/2 alpha lambda
+//       (uR - uL), lambda the larger |u| + c (Rusanov.jl:10-25 at alpha = 1);
+//       params: alpha (default 1).
+//   numerical_flux_method "flux_hllc"  (1D) the HLLC flux (HLLC.jl:9-69)
+//       whatever the scheme's flux.
+//       Both replace the interface flux of every 1D interface, boundary
+//       interfaces included, as the reference's _resolve_flux does
+//       (src/fr/Residual.jl:9-15, :36-46); the 2D residual never consults
+//       the override (Residual2D.jl calls interface_flux_n! directly), so on a
+//       2D solve the slot is accepted and has no effect, as there.
 //   post_step "positivity_zhang_shu"  the positivity-preserving scaling of
 //       Zhang & Shu (J. Comput. Phys. 229 (2010) 8918-8934): per element,
 //       the density at every solution point is pulled toward the element
@@ -41,6 +52,8 @@ struct HookEntry {
 };
 const HookEntry kHooks[] = {
     {"positivity_zhang_shu", FRG_HOOK_POST_STEP, kHookPositivity, 2},
+    {"flux_rusanov", FRG_HOOK_NUMERICAL_FLUX, kHookFluxRusanov, 1},
+    {"flux_hllc", FRG_HOOK_NUMERICAL_FLUX, kHookFluxHLLC, 0},
 };
 constexpr int kNumHooks = (int)(sizeof(kHooks) / sizeof(kHooks[0]));
 
@@ -234,8 +247,38 @@ int frg_hook_lookup(const char* name, int* slot, int* id) {
   return FRG_ERR_UNSUPPORTED_HOOK;
 }
 
+// numerical_flux_method slot: the 1D interface flux of the solve (the 2D
+// residual ignores overrides, as the reference's does)
+static int set_flux_hook(frg_solve* s, int id, const double* params, int nparams) {
+  int found = -1;
+  for (int i = 0; i < kNumHooks; ++i)
+    if (kHooks[i].slot == FRG_HOOK_NUMERICAL_FLUX && kHooks[i].id == id) found = i;
+  if (id != 0 && found < 0) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook implementation");
+  if (id != 0 && (nparams < 0 || nparams > kHooks[found].nparams || (nparams > 0 && !params)))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters");
+  double alpha = 1.0;
+  if (id == kHookFluxRusanov && nparams > 0) alpha = params[0];
+  if (!(alpha >= 0.0) || !std::isfinite(alpha)) return set_err(s->ctx, FRG_ERR_INVALID_ARG, "alpha must be >= 0");
+  s->flux_hook_id = id;
+  s->flux_hook_alpha = alpha;
+  if (s->dim == 1) {
+    s->L1.flux = id == kHookFluxRusanov ? FRG_FLUX_RUSANOV : (id == kHookFluxHLLC ? FRG_FLUX_HLLC : s->scheme_flux);
+    s->L1.phys.flux_alpha = id == kHookFluxRusanov ? alpha : 1.0;
+  }
+  return FRG_OK;
+}
+
 int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams) {
   if (!s) return FRG_ERR_INVALID_ARG;
+  if (slot == FRG_HOOK_NUMERICAL_FLUX) {
+    const int rc = set_flux_hook(s, id, params, nparams);
+    if (rc) return rc;
+    if (s->graph) {  // captured step graphs bake the flux kernels in
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    return FRG_OK;
+  }
   if (slot != FRG_HOOK_POST_STEP) return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook slot");
   if (id == 0) {
     s->post_step_id = 0;

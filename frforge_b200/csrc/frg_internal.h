@@ -110,7 +110,12 @@ struct DevScalars {
 enum : int { kRunning = 0, kFinished = 3 };
 
 // device hook implementations (frg_hooks.cu)
-enum : int { kHookNone = 0, kHookPositivity = 1 };
+enum : int {
+  kHookNone = 0,
+  kHookPositivity = 1,       // post_step: Zhang-Shu positivity scaling
+  kHookFluxRusanov = 2,      // numerical_flux: Rusanov, dissipation scaled by a parameter
+  kHookFluxHLLC = 3,         // numerical_flux: HLLC
+};
 
 // Stage kernel launch parameters (shared by the 1D and 2D kernels).
 struct StageBufs {
@@ -136,6 +141,9 @@ enum : int { kModeStage = 0, kModeResidual = 1, kModePrime = 2, kModeSense = 3 }
 struct Phys {
   double gamma, g1;  // gamma, gamma-1
   double c_av, kappa, s0, eps_floor;
+  // 1D interface flux: dissipation scale of the Rusanov flux (1 except under
+  // a numerical_flux_method override that scales it)
+  double flux_alpha;
   int p, pm;  // p, max(p,1)
 };
 

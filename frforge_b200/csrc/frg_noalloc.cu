@@ -172,6 +172,7 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
     o.sdiv = b.sdiv == 0.0 ? 1.0 : b.sdiv;
   }
   Phys& P = L.phys;
+  P.flux_alpha = 1.0;
   P.gamma = d->gamma;
   P.g1 = d->gamma - 1.0;
   P.c_av = d->c_av;

@@ -47,6 +47,9 @@ struct frg_solve {
   double hmin = 0.0;
   int post_step_id = 0;  // device post-step hook (frg_hooks.cu), 0 = none
   double post_step_params[2] = {0.0, 0.0};
+  int scheme_flux = 0;     // the scheme's flux (FRG_FLUX_*)
+  int flux_hook_id = 0;    // numerical_flux_method override (frg_hooks.cu), 0 = none
+  double flux_hook_alpha = 1.0;
 };
 
 

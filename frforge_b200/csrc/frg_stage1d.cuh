@@ -159,7 +159,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
       }
       double fh[3], gh[3] = {0.0, 0.0, 0.0};
       if (eA >= 0 && eB >= 0) {
-        iflux1<FLUX>(P.gamma, P.g1, uA, uB, fh);
+        iflux1<FLUX>(P.gamma, P.g1, uA, uB, fh, P.flux_alpha);
         if (kBR0) {
           const double sa = sEps[sA] / sJ[sA], sb = sEps[sB] / sJ[sB];
           const double tau = br0_tau(sEps[sA], sEps[sB], sDx[sA], sDx[sB], P.p);
@@ -169,7 +169,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
       } else if (eB >= 0) {  // domain left end (Residual.jl:63-89)
         double ug[3];
         exterior1(M.bc[0], uB, -1.0, ug);
-        iflux1<FLUX>(P.gamma, P.g1, ug, uB, fh);
+        iflux1<FLUX>(P.gamma, P.g1, ug, uB, fh, P.flux_alpha);
         if (kBR0) {
           const double sb = sEps[sB] / sJ[sB];
 #pragma unroll
@@ -178,7 +178,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
       } else {  // domain right end (Residual.jl:91-112)
         double ug[3];
         exterior1(M.bc[1], uA, 1.0, ug);
-        iflux1<FLUX>(P.gamma, P.g1, uA, ug, fh);
+        iflux1<FLUX>(P.gamma, P.g1, uA, ug, fh, P.flux_alpha);
         if (kBR0) {
           const double sa = sEps[sA] / sJ[sA];
 #pragma unroll

@@ -164,6 +164,49 @@ class PositivityPreservingPersson(PerssonAVMethod):
         return p
 
 
+class FluxOverridePersson(PerssonAVMethod):
+    """Persson AV whose numerical_flux_method (Interfaces.jl:73-76) replaces
+    the scheme's 1D interface flux: flux="rusanov" gives the Rusanov flux
+    with its dissipation scaled by alpha, 1/2 (F(uL) + F(uR)) - 1/2 alpha
+    lambda (uR - uL) (alpha = 1: Rusanov.jl:10-25), flux="hllc" the HLLC
+    flux.  A src/methods-style plugin: it names the device implementation of
+    the hook ("flux_rusanov" / "flux_hllc", frg_hooks.cu), so it runs on the
+    GPU.  As in the reference, only the 1D residual consults the override."""
+
+    def __init__(self, flux="rusanov", alpha=1.0, kappa=4.0, s0_factor=-4.0, c_av=0.1,
+                 av_form="conservative_br0"):
+        super().__init__(kappa, s0_factor, c_av, av_form)
+        if flux not in ("rusanov", "hllc"):
+            raise ValueError("flux must be 'rusanov' or 'hllc'")
+        self.flux, self.alpha = flux, float(alpha)
+        self.gpu_hooks = {"numerical_flux_method": (f"flux_{flux}", (self.alpha,) if flux == "rusanov" else ())}
+
+    def numerical_flux_method(self, eq, uL, uR):
+        """Host restatement (1D Euler, conserved (rho, rho u, E))."""
+        import numpy as np
+
+        if self.flux == "hllc":
+            raise NotImplementedError("the HLLC override is evaluated by the GPU stage kernel")
+        uL, uR = np.asarray(uL, dtype=np.float64), np.asarray(uR, dtype=np.float64)
+
+        def flux(U):
+            u = U[1] / U[0]
+            r = max(U[0], np.finfo(np.float64).eps)
+            p = (eq.gamma - 1.0) * (U[2] - 0.5 * r * (U[1] / r) ** 2)
+            return np.array([U[1], U[1] * u + p, (U[2] + p) * u]), abs(U[1] / r) + np.sqrt(
+                eq.gamma * max(p, np.finfo(np.float64).eps) / r)
+
+        fL, sL = flux(uL)
+        fR, sR = flux(uR)
+        lam = self.alpha * max(sL, sR)
+        return 0.5 * (fL + fR) - 0.5 * lam * (uR - uL)
+
+    def method_params(self):
+        p = super().method_params()
+        p.update({"method": "persson_av_flux_override", "flux": self.flux, "alpha": self.alpha})
+        return p
+
+
 _GPU_CLASSES = (ScaledPerssonMethod, PerssonAVMethod, NullCapturing)
 
 # Method registry (Interfaces.jl:118-135, src/methods/Registry.jl:14-53)
@@ -172,6 +215,7 @@ METHOD_REGISTRY: Dict[str, Callable[..., AbstractCapturingMethod]] = {
     "persson_av": lambda **kw: PerssonAVMethod(**kw),
     "scaled_persson": lambda **kw: ScaledPerssonMethod(**kw),
     "persson_av_positive": lambda **kw: PositivityPreservingPersson(**kw),
+    "persson_av_flux_override": lambda **kw: FluxOverridePersson(**kw),
 }
 
 

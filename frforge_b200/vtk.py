@@ -18,6 +18,11 @@ reference writes them:
 Every element owns its nodes (face nodes duplicated), so jumps between
 elements are kept.  Values are written in the shortest decimal form that
 reads back to the same double.
+
+With ``solve=`` (a GpuSolve of the state), the node coordinates, the
+interpolation and the Euler point fields are evaluated on the device from
+the solve's current state (frg_vtk_point_data); only the node data is
+downloaded.
 """
 from __future__ import annotations
 
@@ -152,11 +157,65 @@ def _physical_xy(mesh, xi: np.ndarray, eta: np.ndarray):
     return X, Y
 
 
+def device_point_data(solve, state):
+    """(coords [n_points, 3], {field: values}) of the VTU nodes, evaluated on
+    the device from the solve's current state (frg_vtk_point_data)."""
+    import ctypes as C
+
+    from . import _lib as L
+
+    p = state.ops.p
+    if state.dim == 1:
+        xi = vtk_lagrange_line_nodes(p)
+        eta = None
+        names = ["rho", "u", "p", "rho_u", "E"]
+    else:
+        nodes = vtk_lagrange_quad_nodes(p)
+        xi = np.array([a for a, _ in nodes])
+        eta = np.ascontiguousarray([b for _, b in nodes], dtype=np.float64)
+        names = ["rho", "u", "v", "p", "rho_u", "rho_v", "E"]
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    n_per = xi.size
+    n_pts = state.mesh.n_elements * n_per
+    nc = 1 if state.dim == 1 else 2
+    xy = np.empty(nc * n_pts)
+    f = np.empty(len(names) * n_pts)
+    L.check(L.load().frg_vtk_point_data(solve.handle, n_per, L.dptr(xi), L.dptr(eta) if eta is not None else None,
+                                        L.dptr(xy), L.dptr(f), n_pts), solve.ctx.handle, "frg_vtk_point_data")
+    coords = np.zeros((n_pts, 3))
+    coords[:, 0] = xy[:n_pts]
+    if nc == 2:
+        coords[:, 1] = xy[n_pts:]
+    return coords, {n: f[k * n_pts:(k + 1) * n_pts] for k, n in enumerate(names)}
+
+
 def write_vtu_high_order(path: str, state, eq, cell_fields: Optional[Dict[str, np.ndarray]] = None,
-                         point_fields: Optional[Dict[str, np.ndarray]] = None) -> str:
-    """write_vtu_high_order(path, state, eq; cell_fields, point_fields)."""
+                         point_fields: Optional[Dict[str, np.ndarray]] = None, solve=None) -> str:
+    """write_vtu_high_order(path, state, eq; cell_fields, point_fields); with
+    solve= the point data comes from the device state of that GpuSolve."""
     ops, mesh = state.ops, state.mesh
     p = ops.p
+    if solve is not None and isinstance(eq, (Euler1D, Euler2D)):
+        coords, fields = device_point_data(solve, state)
+        names = list(fields)
+        n_per = p + 1 if state.dim == 1 else (p + 1) ** 2
+        Nel = mesh.n_elements
+        n_pts = Nel * n_per
+        for name, vec in (point_fields or {}).items():
+            vec = np.asarray(vec, dtype=np.float64).ravel()
+            if vec.size != n_pts:
+                raise ValueError(f"point field {name} length {vec.size} != n_pts {n_pts}")
+            fields[name] = vec
+        cell_data = {}
+        for name, vec in (cell_fields or {}).items():
+            vec = np.asarray(vec, dtype=np.float64).ravel()
+            if vec.size != Nel:
+                raise ValueError(f"cell field {name} length {vec.size} != Nel {Nel}")
+            cell_data[name] = vec
+            fields[name] = np.repeat(vec, n_per)
+        names = names + sorted(n for n in fields if n not in names)
+        ctype = VTK_LAGRANGE_LINE if state.dim == 1 else VTK_LAGRANGE_QUAD
+        return _write(path, coords, Nel, n_per, ctype, fields, names, cell_data or None)
     if state.dim == 1:
         Nel = mesh.n_elements
         I = gl_to_equi_interp(ops)

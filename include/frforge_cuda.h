@@ -374,6 +374,19 @@ typedef struct frg_diagnostics {
 int frg_diagnostics_compute(frg_solve* s, int exact, const double* ref_dev, double t_exact, int c,
                             frg_diagnostics* out);
 
+/* Point data of the high-order VTU writer (write_vtu_high_order,
+   src/io/VTKHighOrder.jl:325-535) evaluated on the device from the current
+   state: n_per = (p+1)^dim VTK Lagrange nodes per element given as reference
+   coordinates node_xi / node_eta (eta: 2D only) in VTK node order; the state
+   is interpolated from the solution points with the Lagrange basis at each
+   node.  Host outputs, field-major over n_points = nel * n_per nodes
+   (element-major): xy = x (and y in 2D) from physical_xy including the
+   analytic wavy map; fields = rho, u, v, p, rho_u, rho_v, E (2D) or rho, u,
+   p, rho_u, E (1D).  2D meshes with caller metrics (no node coordinates)
+   are rejected with FRG_ERR_INVALID_ARG. */
+int frg_vtk_point_data(frg_solve* s, int n_per, const double* node_xi, const double* node_eta,
+                       double* xy, double* fields, size_t n_points);
+
 /* Device-side diagnostics of a delivered server request's final state (see
    frg_diagnostics_compute; no exact solution).  FRG_ERR_STATE before the
    request completed successfully. */
@@ -463,16 +476,22 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
    (no counterpart in the reference, whose hooks are Julia methods:
    src/capturing/Interfaces.jl:43-92).  Slots: post_step (called after every
    completed step, before the next compute_dt, as post_step! in
-   ssp_rk3_step!, SSP_RK3.jl:162).  Implementations:
+   ssp_rk3_step!, SSP_RK3.jl:162); numerical_flux_method (the flux of every
+   1D interface, boundary interfaces included, as _resolve_flux,
+   src/fr/Residual.jl:9-15; the 2D residual ignores it, as the reference's
+   does).  Implementations:
      "positivity_zhang_shu"  post_step: the positivity-preserving scaling of
         Zhang & Shu (J. Comput. Phys. 229, 2010) toward the element mean,
         density >= params[0], pressure >= params[1] (default 1e-13 each);
         element integrals are unchanged.
+     "flux_rusanov"  numerical_flux_method: Rusanov with its dissipation
+        scaled by params[0] = alpha >= 0 (default 1, the reference's flux).
+     "flux_hllc"  numerical_flux_method: HLLC whatever the scheme's flux.
    Batched instances run their hooks too: set one on the slot's solve
    (frg_batch_get_solve) before frg_batch_start, or on a queued request with
    frg_server_set_hook; the batch groups instances by hook and steps them
    to the same results as a single solve. */
-enum { FRG_HOOK_POST_STEP = 0 };
+enum { FRG_HOOK_POST_STEP = 0, FRG_HOOK_NUMERICAL_FLUX = 1 };
 int frg_hook_count(void);
 int frg_hook_info(int index, const char** name, int* slot, int* id, int* nparams);
 /* FRG_ERR_UNSUPPORTED_HOOK if no implementation has that name. */

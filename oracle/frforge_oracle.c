@@ -369,6 +369,8 @@ struct orc_solver {
   double gamma;
   int flux, time_scheme, method, av_form;
   double kappa, s0_factor, eps_floor, c_av;
+  int flux_override;  /* numerical_flux_method override (1D): -1 none, else ORC_FLUX_* */
+  double flux_alpha;  /* its Rusanov dissipation scale */
   orc_bc bc[4]; /* 1D: [0]=left [1]=right; 2D: left right bottom top */
   double t;
   /* 1D mesh */
@@ -443,6 +445,8 @@ orc_solver* orc_create_1d(int p, int points, int nel, double xl, double xr,
   s->neq = 3;
   s->gamma = gamma;
   s->flux = flux;
+  s->flux_override = -1;
+  s->flux_alpha = 1.0;
   s->time_scheme = time_scheme;
   s->method = method;
   s->av_form = av_form;
@@ -694,6 +698,8 @@ orc_solver* orc_create_2d(int p, int points, int nx, int ny, double xl,
   s->neq = 4;
   s->gamma = gamma;
   s->flux = flux;
+  s->flux_override = -1;
+  s->flux_alpha = 1.0;
   s->time_scheme = time_scheme;
   s->method = method;
   s->av_form = av_form;
@@ -828,13 +834,18 @@ static inline void pflux1(double g, const double* U, double* f) {
   f[1] = ru * u + p;
   f[2] = (E + p) * u;
 }
-/* rusanov_flux, src/flux/Rusanov.jl:10-25 with max_wave_speed Euler.jl:107-113 */
-void orc_rusanov_1d(double g, const double* uL, const double* uR, double* out) {
+/* rusanov_flux, src/flux/Rusanov.jl:10-25 with max_wave_speed Euler.jl:107-113;
+   alpha scales the dissipation (1 for the reference's flux, exactly) */
+static void rusanov_1d_scaled(double g, const double* uL, const double* uR, double alpha, double* out) {
   double fl[3], fr[3];
   pflux1(g, uL, fl);
   pflux1(g, uR, fr);
   double lam = jmax(fabs(velocity1(uL)) + sound1(g, uL), fabs(velocity1(uR)) + sound1(g, uR));
+  lam = alpha * lam;
   for (int c = 0; c < 3; ++c) out[c] = 0.5 * (fl[c] + fr[c]) - 0.5 * lam * (uR[c] - uL[c]);
+}
+void orc_rusanov_1d(double g, const double* uL, const double* uR, double* out) {
+  rusanov_1d_scaled(g, uL, uR, 1.0, out);
 }
 /* hllc_flux, src/flux/HLLC.jl:9-69 */
 void orc_hllc_1d(double g, const double* uL, const double* uR, double* out) {
@@ -869,11 +880,23 @@ void orc_hllc_1d(double g, const double* uL, const double* uR, double* out) {
   double Us[3] = {factor, factor * SM, factor * e_int};
   for (int c = 0; c < 3; ++c) out[c] = F[c] + S * (Us[c] - U[c]);
 }
+/* _resolve_flux (src/fr/Residual.jl:9-15): the method's numerical_flux_method
+   override when it has one, else the scheme's interface_flux */
 static inline void iflux1(const orc_solver* s, const double* um, const double* up, double* out) {
-  if (s->flux == ORC_FLUX_HLLC)
+  const int kind = s->flux_override >= 0 ? s->flux_override : s->flux;
+  if (kind == ORC_FLUX_HLLC)
     orc_hllc_1d(s->gamma, um, up, out);
   else
-    orc_rusanov_1d(s->gamma, um, up, out);
+    rusanov_1d_scaled(s->gamma, um, up, s->flux_override >= 0 ? s->flux_alpha : 1.0, out);
+}
+
+/* A 1D method's numerical_flux_method override (plugin fluxes of the
+   checker): kind -1 clears it; ORC_FLUX_RUSANOV with its dissipation scaled
+   by alpha; ORC_FLUX_HLLC.  The 2D residual ignores overrides, as the
+   reference's does. */
+void orc_set_flux_override(orc_solver* s, int kind, double alpha) {
+  s->flux_override = kind;
+  s->flux_alpha = alpha;
 }
 
 /* ------------------------------------------------------------- Euler 2D */

@@ -129,6 +129,10 @@ double orc_l2_error_vortex(const orc_solver* s, double t);
 double orc_l2_error_smooth_2d(const orc_solver* s, double t);
 double orc_l2_error_density_wave_1d(const orc_solver* s, double t);
 
+/* numerical_flux_method override of the 1D residual: kind -1 none,
+   ORC_FLUX_RUSANOV (dissipation scaled by alpha) or ORC_FLUX_HLLC */
+void orc_set_flux_override(orc_solver* s, int kind, double alpha);
+
 /* single-interface fluxes (unit checks) */
 void orc_hllc_1d(double gamma, const double* uL, const double* uR, double* out);
 void orc_rusanov_1d(double gamma, const double* uL, const double* uR,

@@ -110,6 +110,7 @@ def lib():
         L.orc_metric.argtypes = [C.c_void_p, C.c_char_p]
         L.orc_physical_coords.argtypes = [C.c_void_p, dp, dp]
         L.orc_set_threads.argtypes = [ip]
+        L.orc_set_flux_override.argtypes = [C.c_void_p, ip, C.c_double]
         L.orc_residual.argtypes = [C.c_void_p, dp]
         L.orc_sense.argtypes = [C.c_void_p, dp]
         L.orc_compute_dt.restype = C.c_double
@@ -257,6 +258,12 @@ class OracleSolver:
                 y.reshape(self.np, self.np, self.nel, order="F"))
 
     # -- hot path --------------------------------------------------------
+    def set_flux_override(self, kind=None, alpha: float = 1.0) -> None:
+        """A 1D method's numerical_flux_method override: None (the scheme's
+        flux), "rusanov" (dissipation scaled by alpha) or "hllc"."""
+        k = -1 if kind is None else {"rusanov": 0, "hllc": 1}[kind]
+        lib().orc_set_flux_override(self._h, k, float(alpha))
+
     def residual(self) -> np.ndarray:
         du = np.zeros(self.ndof)
         lib().orc_residual(self._h, _dp(du))

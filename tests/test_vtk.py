@@ -143,3 +143,66 @@ def test_write_with_capturing_fields(tmp_path):
     F.sense_(sigma, m, st, eq)
     assert np.array_equal(V.read_point_field(path, "sensor")[::9], sigma)
     assert np.all(sigma >= 0)
+
+
+def _points(text):
+    import re
+
+    m = re.search(r"<Points>\s*<DataArray[^>]*>(.*?)</DataArray>", text, re.S)
+    return np.array([float(v) for v in m.group(1).split()])
+
+
+def _field_close(a, b, tol=1e-14):
+    scale = max(float(np.max(np.abs(b))), 1.0)
+    return float(np.max(np.abs(a - b))) / scale <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("wavy", [None, 0.05])
+def test_device_point_data_matches_host_2d(tmp_path, p, wavy):
+    # the node coordinates, GL -> VTK-node interpolation and Euler point fields
+    # evaluated on the device from the solve's state equal the host writer's
+    from frforge_b200.workloads import four_quadrant_ic, four_quadrant_states
+
+    eq = F.Euler2D(1.4)
+    ops = F.build_operators(p)
+    bcs = [F.PeriodicBC() for _ in range(4)]
+    mesh = F.make_wavy_mesh2d(7, 5, amp=wavy, left_bc=bcs[0], right_bc=bcs[1], bottom_bc=bcs[2],
+                              top_bc=bcs[3]) if wavy else F.Mesh2D(0.0, 1.0, 0.0, 1.0, 7, 5, *bcs)
+    st = F.allocate_state(mesh, ops, 4)
+    X, Y = mesh.physical_coords(ops)
+    st.u[...] = four_quadrant_ic(X, Y, four_quadrant_states(5, 0.25))
+    st.u[..., 0] *= 1.0 + 0.1 * np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y)
+    solve = F.GpuSolve(st, eq, F.NullCapturing())
+    solve.upload(st.u, 0.0)
+    host = V.write_vtu_high_order(str(tmp_path / "host.vtu"), st, eq)
+    dev = V.write_vtu_high_order(str(tmp_path / "dev.vtu"), st, eq, solve=solve)
+    hi, di = V.parse_vtu_basic(host), V.parse_vtu_basic(dev)
+    assert hi["n_points"] == di["n_points"] and hi["types"] == di["types"]
+    assert hi["connectivity"] == di["connectivity"]
+    coords_h, _ = V.device_point_data(solve, st)  # also directly
+    for name in ("rho", "u", "v", "p", "rho_u", "rho_v", "E"):
+        assert _field_close(V.read_point_field(dev, name), V.read_point_field(host, name)), name
+    assert _field_close(_points(di["text"]), _points(hi["text"]))
+    assert coords_h.shape == (di["n_points"], 3)
+    solve.close()
+
+
+@pytest.mark.gpu
+def test_device_point_data_matches_host_1d(tmp_path):
+    eq = F.Euler1D(1.4)
+    p = 3
+    ops = F.build_operators(p)
+    mesh = F.Mesh1D(0.0, 1.0, 40, F.TransmissiveBC(), F.TransmissiveBC())
+    st = F.allocate_state(mesh, ops, 3)
+    x = mesh.physical_coords(ops)
+    st.u[...] = eq.primitives_to_conserved(1.0 + 0.3 * np.sin(2 * np.pi * x), 0.2 + 0 * x, 1.0 + 0.1 * x)
+    solve = F.GpuSolve(st, eq, F.NullCapturing())
+    solve.upload(st.u, 0.0)
+    host = V.write_vtu_high_order(str(tmp_path / "h.vtu"), st, eq)
+    dev = V.write_vtu_high_order(str(tmp_path / "d.vtu"), st, eq, solve=solve)
+    for name in ("rho", "u", "p", "rho_u", "E"):
+        assert _field_close(V.read_point_field(dev, name), V.read_point_field(host, name)), name
+    assert V.parse_vtu_basic(dev)["connectivity"] == V.parse_vtu_basic(host)["connectivity"]
+    solve.close()
