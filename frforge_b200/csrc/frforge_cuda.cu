@@ -128,6 +128,8 @@ int dev_alloc(frg_solve* s, T** p, size_t n) {
   return FRG_OK;
 }
 
+int alloc_doubles(frg_solve* s, double** p, size_t n) { return dev_alloc(s, p, n); }
+
 template <class T>
 int dev_upload(frg_solve* s, T** p, const T* host, size_t n) {
   int rc = dev_alloc(s, p, n);
@@ -245,8 +247,15 @@ int enqueue_step(frg_solve* s, bool want_lambda, cudaEvent_t* ev = nullptr) {
   const bool rk2 = s->time_scheme == FRG_TIME_SSP_RK2;
   const int ns = rk2 ? 2 : 3;
   for (int stage = 1; stage <= ns; ++stage) {
+    StageBufs b = stage_bufs(s, stage, want_lambda);
+    if (s->pre_id) {
+      // preprocess_state!: the residual of this stage is evaluated on u_work
+      const int prc = enqueue_preprocess(s, b.us, const_cast<double*>(b.eps_in), stage);
+      if (prc) return prc;
+      b.uw = s->Uw;
+    }
     if (ev) cudaEventRecord(ev[2 * (stage - 1)], s->ctx->stream);
-    const int rc = launch(s, stage_bufs(s, stage, want_lambda));
+    const int rc = launch(s, b);
     if (ev) cudaEventRecord(ev[2 * (stage - 1) + 1], s->ctx->stream);
     if (rc) return rc;
   }
@@ -712,8 +721,10 @@ int frg_residual(frg_solve* s, double* du, size_t n) {
   s->hsc->dt = 0.0;
   if ((rc = push_scalars(s))) return rc;
   if ((rc = prime(s, s->cur, false))) return rc;
+  // preprocess_state!: the residual is that of the work state u_work
+  if (s->pre_id && (rc = enqueue_preprocess(s, s->U[s->cur], s->E[s->cur], 0))) return rc;
   StageBufs b{};
-  b.us = s->U[s->cur];
+  b.us = s->pre_id ? s->Uw : s->U[s->cur];
   b.eps_in = s->E[s->cur];
   b.du_out = s->du;
   b.mode = kModeResidual;
@@ -737,8 +748,10 @@ int frg_sense(frg_solve* s, double* sigma, size_t nel) {
   cudaSetDevice(s->ctx->device);
   int rc;
   if (!s->sigma && (rc = dev_alloc(s, &s->sigma, (size_t)s->nel))) return rc;
+  // sense! sees the work state of a preprocess_state hook, as in residual!
+  if (s->pre_id && (rc = enqueue_preprocess(s, s->U[s->cur], s->E[s->cur], 0))) return rc;
   StageBufs b{};
-  b.us = s->U[s->cur];
+  b.us = s->pre_id ? s->Uw : s->U[s->cur];
   b.sigma_out = s->sigma;
   b.mode = kModeSense;
   b.sc = s->sc;
@@ -783,7 +796,7 @@ static int run_steps(frg_solve* s, double t_final, double cfl, double fixed_dt, 
   // a hook-free 1D solve of at most kLoop1DMaxTiles tiles: K steps per launch
   // of one thread-block cluster (loop1d_kernel) instead of a step graph
   bool loop1d = false;
-  if (use_graph && s->dim == 1 && s->post_step_id == kHookNone) {
+  if (use_graph && s->dim == 1 && s->post_step_id == kHookNone && s->pre_id == kHookNone) {
     int tx = 1, ty = 1;
     batch_tile_shape(1, s->np, 0, &tx, &ty);
     loop1d = (s->nel + tx - 1) / tx <= kLoop1DMaxTiles;

@@ -551,6 +551,8 @@ int frg_batch_slot_group(frg_batch* b, int i, int* variant, int* solo) {
 // Configure an instance's run (integrate! arguments) and mark it running.
 int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixed_dt, int64_t max_steps) {
   if (!b || i < 0 || i >= b->cap || !b->slot[i]) return FRG_ERR_INVALID_ARG;
+  if (b->slot[i]->pre_id)
+    return set_err(b->ctx, FRG_ERR_UNSUPPORTED_HOOK, "batched solves do not run preprocess_state hooks");
   frg_solve* s = b->slot[i];
   if (!s->have_state) return set_err(b->ctx, FRG_ERR_STATE, "no state uploaded");
   if (max_steps < 1 || (!(fixed_dt > 0.0) && !(cfl > 0.0))) return set_err(b->ctx, FRG_ERR_INVALID_ARG, "run");

@@ -17,6 +17,16 @@
 //       (src/fr/Residual.jl:9-15, :36-46); the 2D residual never consults
 //       the override (Residual2D.jl calls interface_flux_n! directly), so on a
 //       2D solve the slot is accepted and has no effect, as there.
+//   preprocess_state "preprocess_positivity_zhang_shu"  the same scaling
+//       (below) applied to the work state u_work that the residual is
+//       evaluated on (preprocess_state!, Interfaces.jl:41-46; called first in
+//       residual!, Residual.jl:172, Residual2D.jl:148): before every stage a
+//       kernel writes u_work = the limited copy of the stage state, the
+//       element viscosity is recomputed from it (sense! and the dissipation
+//       take u_work) and the stage kernel evaluates the residual on it, while
+//       the SSP-RK combination, compute_dt and post_step! keep the stage
+//       state itself.  params: eps_rho, eps_p (defaults 1e-13).  Single
+//       solves only: the batched engine refuses it.
 //   post_step "positivity_zhang_shu"  the positivity-preserving scaling of
 //       Zhang & Shu (J. Comput. Phys. 229 (2010) 8918-8934): per element,
 //       the density at every solution point is pulled toward the element
@@ -54,6 +64,7 @@ const HookEntry kHooks[] = {
     {"positivity_zhang_shu", FRG_HOOK_POST_STEP, kHookPositivity, 2},
     {"flux_rusanov", FRG_HOOK_NUMERICAL_FLUX, kHookFluxRusanov, 1},
     {"flux_hllc", FRG_HOOK_NUMERICAL_FLUX, kHookFluxHLLC, 0},
+    {"preprocess_positivity_zhang_shu", FRG_HOOK_PREPROCESS_STATE, kHookPrePositivity, 2},
 };
 constexpr int kNumHooks = (int)(sizeof(kHooks) / sizeof(kHooks[0]));
 
@@ -161,6 +172,35 @@ __global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, do
   zs_element_1d(u, M, W, np, g1, er, ep, e);
 }
 
+// preprocess_state: u_work = the limited copy of the stage state, one thread
+// per element; gated like the stage it precedes (skipped when the step is
+// inactive or an earlier stage flagged a non-finite value: stage_mask as in
+// stage_control), unless `gated` is 0.
+__global__ void zs_preprocess_2d(const double* __restrict__ us, double* __restrict__ uw, const Mesh2Dev M,
+                                 Weights W, int np, double g1, double er, double ep, const DevScalars* sc,
+                                 unsigned stage_mask, int gated) {
+  if (gated && (!sc->active || (sc->flags & stage_mask))) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  const int np2 = np * np;
+  const size_t n = (size_t)M.nel * np2, base = (size_t)e * np2;
+  for (int c = 0; c < 4; ++c)
+    for (int k = 0; k < np2; ++k) uw[c * n + base + k] = us[c * n + base + k];
+  zs_element_2d(uw, M, W, np, g1, er, ep, e);
+}
+
+__global__ void zs_preprocess_1d(const double* __restrict__ us, double* __restrict__ uw, const Mesh1Dev M,
+                                 Weights W, int np, double g1, double er, double ep, const DevScalars* sc,
+                                 unsigned stage_mask, int gated) {
+  if (gated && (!sc->active || (sc->flags & stage_mask))) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= M.nel) return;
+  const size_t n = (size_t)M.nel * np, base = (size_t)e * np;
+  for (int c = 0; c < 3; ++c)
+    for (int k = 0; k < np; ++k) uw[c * n + base + k] = us[c * n + base + k];
+  zs_element_1d(uw, M, W, np, g1, er, ep, e);
+}
+
 // Batched groups: one CTA per TX x TY tile of the group's tile list, one
 // thread per element of the tile; instances whose step did not complete, or
 // that carry no hook, are left alone.  The CTA of an instance's first tile
@@ -210,6 +250,37 @@ int enqueue_post_step_on(frg_solve* s, bool force, cudaStream_t st) {
   return rt::prime_on(s, 0, true, st);
 }
 int enqueue_post_step(frg_solve* s, bool force) { return enqueue_post_step_on(s, force, s->ctx->stream); }
+
+// Enqueue the preprocess_state hook of a solve for the residual of stage
+// `stage` (0: an ungated evaluation outside the time loop) on the state `us`:
+// the work-state kernel, then the element viscosity of the work state into
+// `eps` (the eps the stage kernel reads).  No-op without a hook.
+int enqueue_preprocess(frg_solve* s, const double* us, double* eps, int stage) {
+  if (s->pre_id != kHookPrePositivity) return FRG_OK;
+  cudaStream_t st = s->ctx->stream;
+  const Weights W = weights_of(s->ops);
+  const int threads = 128, blocks = (s->nel + threads - 1) / threads;
+  const double er = s->pre_params[0], ep = s->pre_params[1];
+  const unsigned mask = stage <= 1 ? 0u : (stage == 2 ? 1u : 5u);
+  const int gated = stage > 0 ? 1 : 0;
+  if (s->dim == 2)
+    zs_preprocess_2d<<<blocks, threads, 0, st>>>(us, s->Uw, s->L2.mesh, W, s->np, s->L2.phys.g1, er, ep, s->sc,
+                                                  mask, gated);
+  else
+    zs_preprocess_1d<<<blocks, threads, 0, st>>>(us, s->Uw, s->L1.mesh, W, s->np, s->L1.phys.g1, er, ep, s->sc,
+                                                  mask, gated);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return rt::cuda_err(s->ctx, e, "preprocess hook");
+  if (s->method != FRG_METHOD_PERSSON) return FRG_OK;
+  StageBufs b{};
+  b.us = s->Uw;
+  b.eps_out = eps;
+  b.mode = kModePrime;
+  b.sc = s->sc;
+  b.use_sc = gated;
+  b.stage = stage > 0 ? stage : 1;
+  return rt::launch(s, b);
+}
 
 int enqueue_batch_post_step(const HostOps& ops, int tx, int ty, const BatchInst* insts, const BatchTile* tiles,
                             int ntiles, cudaStream_t st) {
@@ -268,8 +339,38 @@ static int set_flux_hook(frg_solve* s, int id, const double* params, int nparams
   return FRG_OK;
 }
 
+// preprocess_state slot: the work state's buffer is allocated on selection
+static int set_pre_hook(frg_solve* s, int id, const double* params, int nparams) {
+  if (id != 0 && id != kHookPrePositivity)
+    return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook implementation");
+  if (id != 0 && (nparams < 0 || nparams > 2 || (nparams > 0 && !params)))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters");
+  double p[2] = {1e-13, 1e-13};
+  for (int k = 0; k < nparams; ++k) p[k] = params[k];
+  if (id != 0 && (!(p[0] > 0.0) || !(p[1] > 0.0)))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "eps_rho, eps_p must be > 0");
+  if (id != 0 && !s->Uw) {
+    cudaSetDevice(s->ctx->device);
+    const int rc = alloc_doubles(s, &s->Uw, s->ndof);
+    if (rc) return rc;
+  }
+  s->pre_id = id;
+  s->pre_params[0] = p[0];
+  s->pre_params[1] = p[1];
+  return FRG_OK;
+}
+
 int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams) {
   if (!s) return FRG_ERR_INVALID_ARG;
+  if (slot == FRG_HOOK_PREPROCESS_STATE) {
+    const int rc = set_pre_hook(s, id, params, nparams);
+    if (rc) return rc;
+    if (s->graph) {  // captured step graphs do not contain the hook
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    return FRG_OK;
+  }
   if (slot == FRG_HOOK_NUMERICAL_FLUX) {
     const int rc = set_flux_hook(s, id, params, nparams);
     if (rc) return rc;

@@ -115,6 +115,7 @@ enum : int {
   kHookPositivity = 1,       // post_step: Zhang-Shu positivity scaling
   kHookFluxRusanov = 2,      // numerical_flux: Rusanov, dissipation scaled by a parameter
   kHookFluxHLLC = 3,         // numerical_flux: HLLC
+  kHookPrePositivity = 4,    // preprocess_state: Zhang-Shu scaling of the work state
 };
 
 // Stage kernel launch parameters (shared by the 1D and 2D kernels).
@@ -134,6 +135,9 @@ struct StageBufs {
   int use_sc;       // honour DevScalars active/flags (graph execution)
   DevScalars* sc;
   double* sigma_out;  // kModeSense
+  // residual input when a preprocess_state hook is selected (the work state
+  // u_work); null: the residual is evaluated on us itself
+  const double* uw;
 };
 
 enum : int { kModeStage = 0, kModeResidual = 1, kModePrime = 2, kModeSense = 3 };

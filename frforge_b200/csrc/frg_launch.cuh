@@ -139,8 +139,25 @@ int launch2d_var(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
   return (int)cudaGetLastError();
 }
 
+// A stage with a preprocess_state hook (b.uw set): the default tile variant,
+// staging the work state, with the mesh kind read from the descriptor.
+template <int NP, int FLUX, int AV>
+int launch2d_pre(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
+  using VV = typename Variants2D<NP>::template V_<0>;
+  using S = Smem2D<NP, VV::TX, VV::TY, VV::U0S, VV::MINB, VV::NT>;
+  auto kern = stage2d_kernel<NP, FLUX, AV, VV::TX, VV::TY, VV::MINB, VV::U0S, VV::NT, -1, true>;
+  static KernelSetup setup;
+  const int se = setup.ensure(
+      [&] { return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes); });
+  if (se) return se;
+  dim3 grid((L.mesh.nx + VV::TX - 1) / VV::TX, (L.mesh.ny + VV::TY - 1) / VV::TY);
+  kern<<<grid, VV::NT, S::bytes, st>>>(make_ops<NP>(*L.ops), L.mesh, L.phys, b);
+  return (int)cudaGetLastError();
+}
+
 template <int NP, int FLUX, int AV>
 int launch2d_inst(const Launch2D& L, const StageBufs& b, cudaStream_t st) {
+  if (b.uw) return launch2d_pre<NP, FLUX, AV>(L, b, st);
   const int v = (L.variant >= 0 && L.variant < Variants2D<NP>::n) ? L.variant : 0;
   switch (v) {
     case 1:

@@ -50,12 +50,17 @@ struct frg_solve {
   int scheme_flux = 0;     // the scheme's flux (FRG_FLUX_*)
   int flux_hook_id = 0;    // numerical_flux_method override (frg_hooks.cu), 0 = none
   double flux_hook_alpha = 1.0;
+  int pre_id = 0;          // preprocess_state hook (frg_hooks.cu), 0 = none
+  double pre_params[2] = {0.0, 0.0};
+  double* Uw = nullptr;    // the work state u_work of a preprocess_state hook
 };
 
 
 namespace frg {
 namespace rt {
 int set_err(frg_ctx* c, int code, const std::string& msg);
+// a device buffer of n doubles owned by the solve (freed with it)
+int alloc_doubles(frg_solve* s, double** p, size_t n);
 // the descriptor checks of frg_solve_create (c may be null)
 int validate_desc(frg_ctx* c, const frg_solve_desc* d);
 int cuda_err(frg_ctx* c, cudaError_t e, const char* what);
@@ -72,6 +77,10 @@ StageBufs stage_bufs(const frg_solve* s, int stage, bool want_lambda);
 // post-step hook of a solve and the prime pass of its result (frg_hooks.cu),
 // on the solve's stream or on `st`
 int enqueue_post_step(frg_solve* s, bool force);
+// preprocess_state hook of a solve for the residual of stage `stage` (0: an
+// ungated evaluation) on state us: u_work into s->Uw and its element
+// viscosity into eps (frg_hooks.cu); no-op without a hook
+int enqueue_preprocess(frg_solve* s, const double* us, double* eps, int stage);
 int enqueue_post_step_on(frg_solve* s, bool force, cudaStream_t st);
 // post-step hook of the instances of a batched group whose step completed,
 // one CTA per TX x TY tile of the group's tile list (frg_hooks.cu); the

@@ -200,6 +200,8 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
 // to its solve at admission.
 int frg_server_set_hook(frg_server* s, int64_t id, int slot, int hook_id, const double* params, int nparams) {
   if (!s) return FRG_ERR_INVALID_ARG;
+  if (slot == FRG_HOOK_PREPROCESS_STATE)
+    return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "served solves do not run preprocess_state hooks");
   Request* q = nullptr;
   for (Request& r : s->queue)
     if (r.id == id) q = &r;

@@ -102,7 +102,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
     const int s = r / NP, k = r % NP;
     const int el = sEl[s];
     if (el >= 0) {
-      const double* src = &B.us[c * cs + (size_t)el * NP + k];
+      const double* src = &(B.uw ? B.uw : B.us)[c * cs + (size_t)el * NP + k];
       sU[(s * NEQ + c) * NP + k] = COHERENT ? __ldcg(src) : __ldg(src);
     }
   }
@@ -244,7 +244,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
         bad_du |= !isfinite(du);
         continue;
       }
-      const double us = sU[(s * NEQ + c) * NP + k];
+      const double us = B.uw ? __ldcg(&B.us[gi]) : sU[(s * NEQ + c) * NP + k];
       const double u0 = (B.stage == 1) ? us : B.u0[gi];
       const double un = (B.a * u0 + B.b * us) + cdt * du;
       B.uout[gi] = un;

@@ -199,7 +199,9 @@ FRG_DEV void tile_slots(const Mesh2Dev& M, const TileBuf& tb, const int tx0, con
 
 // P0: issue the cp.async copies of a tile (one commit group); the slots of
 // the buffer must be visible to every thread.
-template <int NP, int AV, class S>
+// PRE: a preprocess_state hook is active; the tile stages the work state
+// B.uw (the residual's input) instead of the stage state B.us.
+template <int NP, int AV, class S, bool PRE = false>
 FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb, const StageCtl& c) {
   constexpr int NEQ = 4, NP2 = NP * NP, ES = S::ES, BX = S::BX, BY = S::BY, NSLOT = S::NSLOT;
   constexpr int TX = BX - 2, TY = BY - 2;
@@ -217,7 +219,7 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
       const int el = tb.el[s];
       if (el < 0) continue;
       double* dst = tb.U + s * ES + k;
-      const double* src = B.us + (size_t)el * NP2 + k;
+      const double* src = (PRE ? B.uw : B.us) + (size_t)el * NP2 + k;
 #pragma unroll
       for (int cc = 0; cc < NEQ; ++cc) cp_async8(dst + cc * NP2, src + cc * cs);
     }
@@ -254,7 +256,9 @@ FRG_DEV void tile_issue(const Mesh2Dev& M, const StageBufs& B, const TileBuf& tb
 // holds an element, the tile positions are its own elements, there is no
 // solid element and every face is an interior face, so no slot flag is read
 // and no boundary or wall case is compiled.
-template <int NP, int FLUX, int AV, class S, int WAIT, int CURV = -1, bool INT = false>
+// PRE: the staged state is the work state of a preprocess_state hook; the
+// stage combination reads the stage state itself from global memory.
+template <int NP, int FLUX, int AV, class S, int WAIT, int CURV = -1, bool INT = false, bool PRE = false>
 FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P, const StageBufs& B,
                           const TileBuf& tb, double* smem, const StageCtl& ctl) {
   static_assert(!INT || CURV == 0, "interior tiles are affine");
@@ -590,15 +594,43 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double ghW = kBR0 ? fw[4] : 0.0;
       const double ghE = kBR0 ? fw[FS + 4] : 0.0;
       const double rjx = sRjx[s];
-      const double rJa = curved ? 0.0 : rjx * sRjy[s];
       const double ev = kAV ? (sEps[s] * rjx) * rjx : 0.0;
+      if (!curved) {
+        // affine: the element factors -1/J, eps/J^2 and 1/Jx are folded into
+        // the line data; each output is two short chains (lifts and fluxes,
+        // dissipation) and one add
+        const double sj = -(rjx * sRjy[s]);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+          Fl[k] *= sj;
+          if (kAV) Ul[k] *= ev;
+        }
+        const double LW = kBR0 ? sj * fhW + rjx * ghW : sj * fhW;
+        const double LE = kBR0 ? sj * fhE + rjx * ghE : sj * fhE;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          double r = ops.gL[i] * LW + ops.gR[i] * LE;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) r += ops.Dt[i][k] * Fl[k];
+          double d = 0.0;
+          if (kBR0) {
+#pragma unroll
+            for (int m = 0; m < NP; ++m) d += ops.DtD[i][m] * Ul[m];
+          } else if (AV == kAvDD) {
+#pragma unroll
+            for (int m = 0; m < NP; ++m) d += ops.DD[i][m] * Ul[m];
+          }
+          Fo[i] = kAV ? r + d : r;
+        }
+        continue;
+      }
       const size_t mrow = (size_t)sEl[s] * NP2 + NP * j;
 #pragma unroll
       for (int i = 0; i < NP; ++i) {
         double acc = ops.gL[i] * fhW + ops.gR[i] * fhE;
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[i][k] * Fl[k];
-        const double rJ = curved ? M.m_rJ[mrow + i] : rJa;
+        const double rJ = M.m_rJ[mrow + i];
         double r = -acc * rJ;
         if (kBR0) {
           double av = 0.0;
@@ -645,15 +677,41 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const double ghS = kBR0 ? fs[4] : 0.0;
       const double ghN = kBR0 ? fs[TX * FS + 4] : 0.0;
       const double rjy = sRjy[s];
-      const double rJa = curved ? 0.0 : sRjx[s] * rjy;
       const double ev = kAV ? (sEps[s] * rjy) * rjy : 0.0;
+      if (!curved) {
+        // affine: element factors folded into the line data (as in P3)
+        const double sj = -(sRjx[s] * rjy);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+          Gl[k] *= sj;
+          if (kAV) Ul[k] *= ev;
+        }
+        const double LS = kBR0 ? sj * fhS + rjy * ghS : sj * fhS;
+        const double LN = kBR0 ? sj * fhN + rjy * ghN : sj * fhN;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+          double r = ops.gL[j] * LS + ops.gR[j] * LN;
+#pragma unroll
+          for (int k = 0; k < NP; ++k) r += ops.Dt[j][k] * Gl[k];
+          double d = 0.0;
+          if (kBR0) {
+#pragma unroll
+            for (int m = 0; m < NP; ++m) d += ops.DtD[j][m] * Ul[m];
+          } else if (AV == kAvDD) {
+#pragma unroll
+            for (int m = 0; m < NP; ++m) d += ops.DD[j][m] * Ul[m];
+          }
+          Go[NP * j] = kAV ? r + d : r;
+        }
+        continue;
+      }
       const size_t mbase = (size_t)sEl[s] * NP2 + i;
 #pragma unroll
       for (int j = 0; j < NP; ++j) {
         double acc = ops.gL[j] * fhS + ops.gR[j] * fhN;
 #pragma unroll
         for (int k = 0; k < NP; ++k) acc += ops.Dt[j][k] * Gl[k];
-        const double rJ = curved ? M.m_rJ[mbase + NP * j] : rJa;
+        const double rJ = M.m_rJ[mbase + NP * j];
         double r = -acc * rJ;
         if (kBR0) {
           double av = 0.0;
@@ -699,7 +757,9 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
               B.du_out[gi] = du;
               continue;
             }
-            const double us = sU[s * ES + c * NP2 + k];
+            // with a preprocess_state hook the residual's input is the work
+            // state; the stage combination takes the stage state itself
+            const double us = PRE ? __ldcg(&B.us[gi]) : sU[s * ES + c * NP2 + k];
             const double u0 = (B.stage == 1) ? us : (U0S ? sU0[li] : u0r[it][c]);
             const double un = (B.a * u0 + B.b * us) + cdt * du;
             B.uout[gi] = un;
@@ -863,7 +923,7 @@ FRG_DEV bool tile_is_interior(const Mesh2Dev& M, const int tx0, const int ty0) {
 // One tile of one stage (single buffer).  tx0, ty0: first element of the
 // tile.  Used by stage2d_kernel and by the batched kernels.
 template <int NP, int FLUX, int AV, int TX, int TY, int MINB, bool U0S, int NTHR = kStageThreads,
-          int CURV = -1>
+          int CURV = -1, bool PRE = false>
 __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
                                              const StageBufs& B, const int tx0, const int ty0) {
   using S = Smem2D<NP, TX, TY, U0S, MINB, NTHR>;
@@ -873,19 +933,20 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
   const TileBuf tb = tile_buf<S>(smem);
   tile_slots<S>(M, tb, tx0, ty0, ctl.prime);
   __syncthreads();
-  tile_issue<NP, AV, S>(M, B, tb, ctl);
+  tile_issue<NP, AV, S, PRE>(M, B, tb, ctl);
   if (CURV != 1 && tile_is_interior<TX, TY>(M, tx0, ty0))
-    tile_compute<NP, FLUX, AV, S, 0, 0, true>(ops, M, P, B, tb, smem, ctl);
+    tile_compute<NP, FLUX, AV, S, 0, 0, true, PRE>(ops, M, P, B, tb, smem, ctl);
   else
-    tile_compute<NP, FLUX, AV, S, 0, CURV>(ops, M, P, B, tb, smem, ctl);
+    tile_compute<NP, FLUX, AV, S, 0, CURV, false, PRE>(ops, M, P, B, tb, smem, ctl);
 }
 
 // Single solve, one tile per CTA: the grid covers the mesh with tiles.
 template <int NP, int FLUX, int AV, int TX = Tile2D<NP>::TX, int TY = Tile2D<NP>::TY, int MINB = 2,
-          bool U0S = true, int NTHR = kStageThreads, int CURV = -1>
+          bool U0S = true, int NTHR = kStageThreads, int CURV = -1, bool PRE = false>
 __global__ void __launch_bounds__(NTHR, MINB)
     stage2d_kernel(const OpsT<NP> ops, const Mesh2Dev M, const Phys P, const StageBufs B) {
-  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR, CURV>(ops, M, P, B, blockIdx.x * TX, blockIdx.y * TY);
+  stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR, CURV, PRE>(ops, M, P, B, blockIdx.x * TX,
+                                                                 blockIdx.y * TY);
 }
 
 }  // namespace frg

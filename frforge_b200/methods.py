@@ -164,6 +164,38 @@ class PositivityPreservingPersson(PerssonAVMethod):
         return p
 
 
+class PositivityPreprocessPersson(PerssonAVMethod):
+    """Persson AV whose preprocess_state! (Interfaces.jl:41-46) limits the
+    work state the residual is evaluated on: u_work is the Zhang-Shu
+    positivity-preserving scaling of the stage state, while the SSP-RK
+    combination keeps the stage state itself.  A src/methods-style plugin
+    that names the device implementation of the hook
+    ("preprocess_positivity_zhang_shu", frg_hooks.cu), so it runs on the GPU;
+    preprocess_state_ is the host restatement (frforge_b200.limiters)."""
+
+    def __init__(self, kappa=4.0, s0_factor=-4.0, c_av=0.1, av_form="conservative_br0", eps_rho=1e-13,
+                 eps_p=1e-13):
+        super().__init__(kappa, s0_factor, c_av, av_form)
+        self.eps_rho, self.eps_p = float(eps_rho), float(eps_p)
+        self.gpu_hooks = {"preprocess_state": ("preprocess_positivity_zhang_shu", (self.eps_rho, self.eps_p))}
+
+    def preprocess_state_(self, u_work, state, eq):
+        import copy
+
+        from .limiters import zhang_shu_limit_
+
+        u_work[...] = state.u
+        work = copy.copy(state)
+        work.u = u_work
+        zhang_shu_limit_(work, eq, self.eps_rho, self.eps_p)
+        return u_work
+
+    def method_params(self):
+        p = super().method_params()
+        p.update({"method": "persson_av_preprocess_positive", "eps_rho": self.eps_rho, "eps_p": self.eps_p})
+        return p
+
+
 class FluxOverridePersson(PerssonAVMethod):
     """Persson AV whose numerical_flux_method (Interfaces.jl:73-76) replaces
     the scheme's 1D interface flux: flux="rusanov" gives the Rusanov flux
@@ -216,6 +248,7 @@ METHOD_REGISTRY: Dict[str, Callable[..., AbstractCapturingMethod]] = {
     "scaled_persson": lambda **kw: ScaledPerssonMethod(**kw),
     "persson_av_positive": lambda **kw: PositivityPreservingPersson(**kw),
     "persson_av_flux_override": lambda **kw: FluxOverridePersson(**kw),
+    "persson_av_preprocess_positive": lambda **kw: PositivityPreprocessPersson(**kw),
 }
 
 

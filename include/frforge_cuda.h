@@ -479,7 +479,8 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
    ssp_rk3_step!, SSP_RK3.jl:162); numerical_flux_method (the flux of every
    1D interface, boundary interfaces included, as _resolve_flux,
    src/fr/Residual.jl:9-15; the 2D residual ignores it, as the reference's
-   does).  Implementations:
+   does); preprocess_state (the state the residual is evaluated on).
+   Implementations:
      "positivity_zhang_shu"  post_step: the positivity-preserving scaling of
         Zhang & Shu (J. Comput. Phys. 229, 2010) toward the element mean,
         density >= params[0], pressure >= params[1] (default 1e-13 each);
@@ -487,11 +488,18 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
      "flux_rusanov"  numerical_flux_method: Rusanov with its dissipation
         scaled by params[0] = alpha >= 0 (default 1, the reference's flux).
      "flux_hllc"  numerical_flux_method: HLLC whatever the scheme's flux.
+     "preprocess_positivity_zhang_shu"  preprocess_state: the residual is
+        evaluated on the work state u_work = the Zhang & Shu scaling of the
+        stage state (params as "positivity_zhang_shu"), its element viscosity
+        included, while the SSP-RK combination, compute_dt and post_step keep
+        the stage state (preprocess_state!, Interfaces.jl:41-46, called first
+        in residual!).  Single solves only: frg_batch_start and
+        frg_server_set_hook refuse it with FRG_ERR_UNSUPPORTED_HOOK.
    Batched instances run their hooks too: set one on the slot's solve
    (frg_batch_get_solve) before frg_batch_start, or on a queued request with
    frg_server_set_hook; the batch groups instances by hook and steps them
    to the same results as a single solve. */
-enum { FRG_HOOK_POST_STEP = 0, FRG_HOOK_NUMERICAL_FLUX = 1 };
+enum { FRG_HOOK_POST_STEP = 0, FRG_HOOK_NUMERICAL_FLUX = 1, FRG_HOOK_PREPROCESS_STATE = 2 };
 int frg_hook_count(void);
 int frg_hook_info(int index, const char** name, int* slot, int* id, int* nparams);
 /* FRG_ERR_UNSUPPORTED_HOOK if no implementation has that name. */

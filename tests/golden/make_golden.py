@@ -13,7 +13,8 @@ build container, never on a GPU host):
 * test/data/shu_osher_ref.csv -- the self-generated Shu-Osher density
   reference (p=1, Ne=200, c_av=0.5, CFL 0.1).
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py /path/to/reference
+   or: FRFORGE_REFERENCE=/path/to/reference python tests/golden/make_golden.py
 """
 import json
 import os
@@ -71,4 +72,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FRFORGE_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py /path/to/reference (or set FRFORGE_REFERENCE)")
+    main(ref)
