@@ -670,14 +670,15 @@ def run_served(args):
 
 def run_ncu_target(args):
     """A short, fixed launch sequence for ncu captures: the 512^2 workload
-    (or --n elements per side, same P, flux, method, IC), default tile
-    variant, one prime launch then --steps SSP-RK3 steps with direct
-    launches (begin, stage 1, 2, 3, end per step)."""
+    (or --n elements per side, same P and IC; --flux / --method replace the
+    workload's flux and capturing method), default tile variant, one prime
+    launch (with Persson AV) then --steps SSP-RK3 steps with direct launches
+    (begin, stage 1, 2, 3, end per step)."""
     import frforge_b200 as F
     from frforge_b200.workloads import C3, Workload2D
 
-    w = Workload2D(C3.name, args.n, C3.p, C3.flux, C3.method, C3.c_av, C3.periodic, C3.cfl, C3.steps,
-                   seed=C3.seed, jump_scale=C3.jump_scale)
+    w = Workload2D(C3.name, args.n, C3.p, args.flux or C3.flux, args.method or C3.method, C3.c_av, C3.periodic,
+                   C3.cfl, C3.steps, seed=C3.seed, jump_scale=C3.jump_scale)
     st, method = w.build(F)
     solve = F.GpuSolve(st, F.Euler2D(1.4), method)
     solve.upload(st.u, 0.0)
@@ -698,6 +699,10 @@ def main():
     ap.add_argument("--served-requests", type=int, default=32)
     ap.add_argument("--ncu-target", action="store_true")
     ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--flux", choices=["hllc", "rusanov"], default=None,
+                    help="--ncu-target: numerical flux (default: the workload's, HLLC)")
+    ap.add_argument("--method", choices=["persson_av", "null"], default=None,
+                    help="--ncu-target: capturing method (default: the workload's, Persson AV)")
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--batch-reps", type=int, default=3)
     args = ap.parse_args()
