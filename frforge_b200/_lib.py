@@ -192,6 +192,7 @@ SIGNATURES = {
     "frg_hook_lookup": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "frg_solve_set_hook": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int]),
     "frg_apply_post_step": (C.c_int, [C.c_void_p]),
+    "frg_solve_hook_calls": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.c_int]),
     "frg_server_set_hook": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_int, _dp, C.c_int]),
     "frg_server_submit_ic": (C.c_int, [C.c_void_p, C.POINTER(frg_solve_desc), C.POINTER(frg_ic), C.c_double,
                                        C.c_double, C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]),

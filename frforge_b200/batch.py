@@ -76,6 +76,13 @@ class Batch:
         self._chk(L.load().frg_batch_get_solve(self.handle, int(slot), C.byref(s)), "frg_batch_get_solve")
         return s
 
+    def hook_calls(self, slot: int) -> dict:
+        """Device-counted hook invocations of the slot's instance (see
+        GpuSolve.hook_calls)."""
+        c = (C.c_int64 * 3)()
+        self._chk(L.load().frg_solve_hook_calls(self._solve(slot), c, 3), "frg_solve_hook_calls")
+        return {name: (None if c[i] < 0 else int(c[i])) for name, i in L.HOOK_SLOT.items()}
+
     def add(self, state, eq, method: Optional[AbstractCapturingMethod] = None, time: Optional[str] = None,
             caller_ops=None) -> int:
         """Create an instance for ``state`` (its u and t are uploaded); returns

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -154,7 +155,9 @@ BCDev to_dev(const frg_bc& b) {
 }
 
 int push_scalars(frg_solve* s) {
-  cudaError_t e = cudaMemcpyAsync(s->sc, s->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->ctx->stream);
+  // everything but the device-side hook counters
+  cudaError_t e =
+      cudaMemcpyAsync(s->sc, s->hsc, offsetof(DevScalars, hook_calls), cudaMemcpyHostToDevice, s->ctx->stream);
   return cuda_err(s->ctx, e, "scalars upload");
 }
 int pull_scalars(frg_solve* s) {
@@ -653,6 +656,7 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
     s->hsc->hmin = s->hmin;
     for (int k = 0; k < 3 && !rc; ++k)
       rc = cuda_err(c, cudaMemsetAsync(s->E[k], 0, sizeof(double) * s->nel, c->stream), "memset");
+    if (!rc) rc = cuda_err(c, cudaMemsetAsync(s->sc, 0, sizeof(DevScalars), c->stream), "memset");
     if (!rc) rc = push_scalars(s);
     if (!rc) rc = cuda_err(c, cudaStreamSynchronize(c->stream), "solve setup");
   }

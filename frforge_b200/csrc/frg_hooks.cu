@@ -153,11 +153,19 @@ __device__ void zs_element_1d(double* u, const Mesh1Dev& M, const Weights& W, in
   zs_element<3>(u, n, base, np, ww, g1, er, ep);
 }
 
+// one count per launch that passed its gate (the HookProbeMethod counters of
+// the reference's test/test_capturing.jl:5-41, kept on the device so graph
+// replays count too)
+__device__ __forceinline__ void count_call(DevScalars* sc, int slot) {
+  if (sc && blockIdx.x == 0 && threadIdx.x == 0) sc->hook_calls[slot] += 1;
+}
+
 // one thread per element; `force` ignores the step's completion flag
 __global__ void zs_limiter_2d(double* u, const Mesh2Dev M, Weights W, int np, double g1, double er, double ep,
                               DevScalars* sc, int force) {
   if (!force && !(sc && sc->stepped_ok)) return;
   if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;  // the prime pass recomputes it
+  count_call(sc, FRG_HOOK_POST_STEP);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M.nel) return;
   zs_element_2d(u, M, W, np, g1, er, ep, e);
@@ -167,6 +175,7 @@ __global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, do
                               DevScalars* sc, int force) {
   if (!force && !(sc && sc->stepped_ok)) return;
   if (!force && blockIdx.x == 0 && threadIdx.x == 0) sc->lam_bits = 0ull;
+  count_call(sc, FRG_HOOK_POST_STEP);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M.nel) return;
   zs_element_1d(u, M, W, np, g1, er, ep, e);
@@ -177,9 +186,10 @@ __global__ void zs_limiter_1d(double* u, const Mesh1Dev M, Weights W, int np, do
 // inactive or an earlier stage flagged a non-finite value: stage_mask as in
 // stage_control), unless `gated` is 0.
 __global__ void zs_preprocess_2d(const double* __restrict__ us, double* __restrict__ uw, const Mesh2Dev M,
-                                 Weights W, int np, double g1, double er, double ep, const DevScalars* sc,
+                                 Weights W, int np, double g1, double er, double ep, DevScalars* sc,
                                  unsigned stage_mask, int gated) {
   if (gated && (!sc->active || (sc->flags & stage_mask))) return;
+  count_call(sc, FRG_HOOK_PREPROCESS_STATE);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M.nel) return;
   const int np2 = np * np;
@@ -190,9 +200,10 @@ __global__ void zs_preprocess_2d(const double* __restrict__ us, double* __restri
 }
 
 __global__ void zs_preprocess_1d(const double* __restrict__ us, double* __restrict__ uw, const Mesh1Dev M,
-                                 Weights W, int np, double g1, double er, double ep, const DevScalars* sc,
+                                 Weights W, int np, double g1, double er, double ep, DevScalars* sc,
                                  unsigned stage_mask, int gated) {
   if (gated && (!sc->active || (sc->flags & stage_mask))) return;
+  count_call(sc, FRG_HOOK_PREPROCESS_STATE);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= M.nel) return;
   const size_t n = (size_t)M.nel * np, base = (size_t)e * np;
@@ -210,7 +221,10 @@ __global__ void zs_limiter_batch(const BatchInst* __restrict__ insts, const Batc
   const BatchTile t = tiles[blockIdx.x];
   const BatchInst& I = insts[t.inst];
   if (I.hook != kHookPositivity || !(I.sc && I.sc->stepped_ok)) return;
-  if (t.x0 == 0 && t.y0 == 0 && threadIdx.x == 0) I.sc->lam_bits = 0ull;
+  if (t.x0 == 0 && t.y0 == 0 && threadIdx.x == 0) {
+    I.sc->lam_bits = 0ull;
+    I.sc->hook_calls[FRG_HOOK_POST_STEP] += 1;
+  }
   const double er = I.hook_params[0], ep = I.hook_params[1];
   for (int k = threadIdx.x; k < tx * ty; k += blockDim.x) {
     const int x = t.x0 + k % tx, y = t.y0 + k / tx;
@@ -413,6 +427,19 @@ int frg_apply_post_step(frg_solve* s) {
   if (rc) return rc;
   if ((rc = enqueue_post_step(s, true))) return rc;
   return cuda_err(s->ctx, cudaStreamSynchronize(s->ctx->stream), "post-step hook");
+}
+
+int frg_solve_hook_calls(frg_solve* s, int64_t* counts, int n) {
+  if (!s || !counts || n < 1 || n > 3) return FRG_ERR_INVALID_ARG;
+  cudaSetDevice(s->ctx->device);
+  long long c[3] = {0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(c, s->sc->hook_calls, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
+  if (e != cudaSuccess) return cuda_err(s->ctx, e, "hook counters");
+  for (int i = 0; i < n; ++i) counts[i] = c[i];
+  // the numerical-flux override runs inline in every interface pass: no launch of its own to count
+  if (n > FRG_HOOK_NUMERICAL_FLUX) counts[FRG_HOOK_NUMERICAL_FLUX] = -1;
+  return FRG_OK;
 }
 
 }  // extern "C"

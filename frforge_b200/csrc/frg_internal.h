@@ -105,6 +105,9 @@ struct DevScalars {
   long long n_steps;
   long long max_steps;
   long long residual_evals;
+  // launches of each hook slot's kernel that passed their gate (indexed by
+  // FRG_HOOK_*); counted on the device and never overwritten from the host
+  long long hook_calls[3];
 };
 
 enum : int { kRunning = 0, kFinished = 3 };

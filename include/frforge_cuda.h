@@ -508,6 +508,16 @@ int frg_hook_lookup(const char* name, int* slot, int* id);
 int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int nparams);
 /* Apply the post-step hook once to the current state (host-driven loops). */
 int frg_apply_post_step(frg_solve* s);
+/* Invocation counts of the solve's hooks since frg_solve_create, counted on
+   the device (graph replays and batched steps included), as the counters of
+   HookProbeMethod (test/test_capturing.jl:5-41): counts[FRG_HOOK_POST_STEP]
+   = post-step passes run (one per completed step, plus each
+   frg_apply_post_step), counts[FRG_HOOK_PREPROCESS_STATE] = work states made
+   (one per residual evaluation: stage, frg_residual, frg_sense).  The flux
+   override runs inline in every interface pass, with no launch of its own:
+   counts[FRG_HOOK_NUMERICAL_FLUX] = -1 (frg_solve_info.residual_evals counts
+   the residuals that used it).  n: entries to fill, 1..3. */
+int frg_solve_hook_calls(frg_solve* s, int64_t* counts, int n);
 /* Select hook `id` of `slot` for a request that is still queued (id 0
    removes it); applied to the request's solve at admission.  FRG_ERR_STATE
    once the request was admitted or completed. */
