@@ -13,7 +13,7 @@ from .mesh import (DirichletBC, Mesh1D, Mesh2D, PeriodicBC, ReflectingBC, Transm
                    XSplitGhostBC, is_periodic, julia_range, make_wavy_mesh2d)
 from .methods import (AbstractCapturingMethod, ElementArtificialViscosity, NullCapturing,
                       PerssonAVMethod, PerssonSensor, PositivityPreservingPersson, ScaledPerssonMethod, FluxOverridePersson,
-                      PositivityPreprocessPersson,
+                      PositivityPreprocessPersson, TraceOverridePersson,
                       get_capturing_method, list_methods, method_params, register_method)
 from .operators import FROperators, build_operators, n_points
 from .scheme import DEFAULT_SCHEME, SchemeConfig, parse_scheme, scheme_dict

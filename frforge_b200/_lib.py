@@ -118,7 +118,7 @@ def make_ic(kind: str, prim=(), x0: float = 0.5, y0: float = 0.5, amp: float = 0
     return ic
 
 
-HOOK_SLOT = {"post_step": 0, "numerical_flux_method": 1, "preprocess_state": 2}
+HOOK_SLOT = {"post_step": 0, "numerical_flux_method": 1, "preprocess_state": 2, "extrapolate_interface": 3}
 
 
 def device_hooks() -> dict:

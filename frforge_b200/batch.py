@@ -79,8 +79,8 @@ class Batch:
     def hook_calls(self, slot: int) -> dict:
         """Device-counted hook invocations of the slot's instance (see
         GpuSolve.hook_calls)."""
-        c = (C.c_int64 * 3)()
-        self._chk(L.load().frg_solve_hook_calls(self._solve(slot), c, 3), "frg_solve_hook_calls")
+        c = (C.c_int64 * len(L.HOOK_SLOT))()
+        self._chk(L.load().frg_solve_hook_calls(self._solve(slot), c, len(c)), "frg_solve_hook_calls")
         return {name: (None if c[i] < 0 else int(c[i])) for name, i in L.HOOK_SLOT.items()}
 
     def add(self, state, eq, method: Optional[AbstractCapturingMethod] = None, time: Optional[str] = None,

@@ -620,6 +620,9 @@ int frg_solve_create(frg_ctx* c, const frg_solve_desc* d, frg_solve** out) {
   }
   Phys P;
   P.flux_alpha = 1.0;
+  P.trace_hook = 0;
+  P.trace_p0 = 0.0;
+  P.trace_p1 = 0.0;
   P.gamma = d->gamma;
   P.g1 = d->gamma - 1.0;
   P.c_av = d->c_av;

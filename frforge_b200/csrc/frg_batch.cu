@@ -565,7 +565,9 @@ int frg_batch_start(frg_batch* b, int i, double t_final, double cfl, double fixe
   // a hook selected after the last rebuild regroups the instance
   const BatchInst I = inst_of(s);
   if (i >= (int)b->h_insts.size() || b->h_insts[i].hook != I.hook ||
-      b->h_insts[i].hook_params[0] != I.hook_params[0] || b->h_insts[i].hook_params[1] != I.hook_params[1])
+      b->h_insts[i].hook_params[0] != I.hook_params[0] || b->h_insts[i].hook_params[1] != I.hook_params[1] ||
+      b->h_insts[i].P.flux_alpha != I.P.flux_alpha || b->h_insts[i].P.trace_hook != I.P.trace_hook ||
+      b->h_insts[i].P.trace_p0 != I.P.trace_p0 || b->h_insts[i].P.trace_p1 != I.P.trace_p1)
     b->dirty = true;
   b->running[i] = 1;
   return FRG_OK;

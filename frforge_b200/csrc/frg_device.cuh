@@ -461,6 +461,67 @@ FRG_DEV double br0_tau(double em, double ep, double hm, double hp, int p) {
   return 2.0 * eb * (double)(p + 1) * frcp(jmax(hb, kEps));
 }
 
+// smallest root in [0, 1] of a t^2 + b t + c with c > 0 >= a + b + c (the
+// pressure quadratic of the Zhang-Shu scaling)
+FRG_DEV double root01(double a, double b, double c) {
+  if (fabs(a) < 1e-300) return b != 0.0 ? fmin(fmax(-c / b, 0.0), 1.0) : 0.0;
+  const double disc = fmax(b * b - 4.0 * a * c, 0.0);
+  const double q = -0.5 * (b + copysign(sqrt(disc), b));
+  double r1 = q / a, r2 = q != 0.0 ? c / q : 2.0;
+  double t = 1.0;
+  if (r1 >= 0.0 && r1 <= 1.0) t = fmin(t, r1);
+  if (r2 >= 0.0 && r2 <= 1.0) t = fmin(t, r2);
+  return t;
+}
+
+// extrapolate_interface override of a 1D element (Interfaces.jl:49-71 is the
+// default, "Override for hybrid reconstruction"): given the element mean m
+// and its Lagrange traces tl (xi = -1) and tr (xi = +1) of (rho, rho u, E),
+// kind kHookTraceMean pulls both toward the mean, t = m + p0 (t - m);
+// kind kHookTracePositivity applies the Zhang-Shu scaling to the two traces
+// (density >= p0 first, then pressure >= p1 by the pressure quadratic's root
+// along m + theta (t - m)), and leaves an element whose mean is not
+// admissible as it is.
+FRG_DEV void trace_override1(int kind, double p0, double p1, double g1, const double* m, double* tl, double* tr) {
+  if (kind == kHookTraceMean) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      tl[c] = m[c] + p0 * (tl[c] - m[c]);
+      tr[c] = m[c] + p0 * (tr[c] - m[c]);
+    }
+    return;
+  }
+  if (kind != kHookTracePositivity) return;
+  const double er = p0, ep = p1;
+  const double pbar = g1 * (m[2] - 0.5 * m[1] * m[1] / m[0]);
+  if (!(m[0] > er) || !(pbar > ep)) return;
+  const double rmin = fmin(tl[0], tr[0]);
+  if (rmin < er) {
+    const double th = (m[0] - er) / (m[0] - rmin);
+    tl[0] = m[0] + th * (tl[0] - m[0]);
+    tr[0] = m[0] + th * (tr[0] - m[0]);
+  }
+  double theta = 1.0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const double* U = side == 0 ? tl : tr;
+    const double pk = g1 * (U[2] - 0.5 * U[1] * U[1] / U[0]);
+    if (pk >= ep) continue;
+    const double d0 = U[0] - m[0], d1 = U[1] - m[1], d2 = U[2] - m[2];
+    const double a = g1 * (d2 * d0 - 0.5 * d1 * d1);
+    const double b = g1 * (m[2] * d0 + m[0] * d2 - m[1] * d1) - ep * d0;
+    const double cc = m[0] * (pbar - ep);
+    theta = fmin(theta, root01(a, b, cc));
+  }
+  if (theta < 1.0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      tl[c] = m[c] + theta * (tl[c] - m[c]);
+      tr[c] = m[c] + theta * (tr[c] - m[c]);
+    }
+  }
+}
+
 // atomic max of a non-negative double via its bit pattern (NaN sorts high)
 FRG_DEV void atomic_max_nonneg(unsigned long long* addr, double v) {
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));

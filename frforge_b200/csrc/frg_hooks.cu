@@ -17,6 +17,18 @@
 //       (src/fr/Residual.jl:9-15, :36-46); the 2D residual never consults
 //       the override (Residual2D.jl calls interface_flux_n! directly), so on a
 //       2D solve the slot is accepted and has no effect, as there.
+//   extrapolate_interface "traces_toward_mean"  (1D) the traces of every
+//       element's numerical fluxes pulled toward its mean, ubar + theta
+//       (ell . u - ubar) (theta = 1: the Lagrange traces of the default
+//       extrapolate_interface!, Interfaces.jl:49-71; theta = 0: first-order
+//       traces); params: theta in [0, 1] (default 1).
+//   extrapolate_interface "traces_positivity_zhang_shu"  (1D) the
+//       Zhang-Shu scaling (below) applied to an element's two traces; params:
+//       eps_rho, eps_p (defaults 1e-13).
+//       Both feed only compute_interface_fluxes! (Residual.jl:175-184); the
+//       BR0 dissipation keeps the Lagrange traces, as apply_dissipation_br0!
+//       computes its own (PerssonAV.jl:249-300).  The 2D residual never calls
+//       extrapolate_interface!, so on a 2D solve the slot has no effect.
 //   preprocess_state "preprocess_positivity_zhang_shu"  the same scaling
 //       (below) applied to the work state u_work that the residual is
 //       evaluated on (preprocess_state!, Interfaces.jl:41-46; called first in
@@ -65,24 +77,14 @@ const HookEntry kHooks[] = {
     {"flux_rusanov", FRG_HOOK_NUMERICAL_FLUX, kHookFluxRusanov, 1},
     {"flux_hllc", FRG_HOOK_NUMERICAL_FLUX, kHookFluxHLLC, 0},
     {"preprocess_positivity_zhang_shu", FRG_HOOK_PREPROCESS_STATE, kHookPrePositivity, 2},
+    {"traces_toward_mean", FRG_HOOK_EXTRAPOLATE_INTERFACE, kHookTraceMean, 1},
+    {"traces_positivity_zhang_shu", FRG_HOOK_EXTRAPOLATE_INTERFACE, kHookTracePositivity, 2},
 };
 constexpr int kNumHooks = (int)(sizeof(kHooks) / sizeof(kHooks[0]));
 
 struct Weights {
   double w[kMaxNp];
 };
-
-// smallest root in [0, 1] of a t^2 + b t + c with c > 0 >= a + b + c
-__device__ double root01(double a, double b, double c) {
-  if (fabs(a) < 1e-300) return b != 0.0 ? fmin(fmax(-c / b, 0.0), 1.0) : 0.0;
-  const double disc = fmax(b * b - 4.0 * a * c, 0.0);
-  const double q = -0.5 * (b + copysign(sqrt(disc), b));
-  double r1 = q / a, r2 = q != 0.0 ? c / q : 2.0;
-  double t = 1.0;
-  if (r1 >= 0.0 && r1 <= 1.0) t = fmin(t, r1);
-  if (r2 >= 0.0 && r2 <= 1.0) t = fmin(t, r2);
-  return t;
-}
 
 template <int NEQ>
 __device__ void zs_element(double* u, size_t n, size_t base, int npts, const double* ww, double g1, double er,
@@ -353,6 +355,31 @@ static int set_flux_hook(frg_solve* s, int id, const double* params, int nparams
   return FRG_OK;
 }
 
+// extrapolate_interface slot: the traces of the 1D numerical fluxes (the 2D
+// residual never calls extrapolate_interface!, so a 2D solve ignores it)
+static int set_trace_hook(frg_solve* s, int id, const double* params, int nparams) {
+  if (id != 0 && id != kHookTraceMean && id != kHookTracePositivity)
+    return set_err(s->ctx, FRG_ERR_UNSUPPORTED_HOOK, "unknown hook implementation");
+  const int maxp = id == kHookTraceMean ? 1 : 2;
+  if (id != 0 && (nparams < 0 || nparams > maxp || (nparams > 0 && !params)))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "hook parameters");
+  double p[2] = {id == kHookTraceMean ? 1.0 : 1e-13, 1e-13};
+  for (int k = 0; k < nparams; ++k) p[k] = params[k];
+  if (id == kHookTraceMean && !(p[0] >= 0.0 && p[0] <= 1.0))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "theta must be in [0, 1]");
+  if (id == kHookTracePositivity && (!(p[0] > 0.0) || !(p[1] > 0.0) || !std::isfinite(p[0]) || !std::isfinite(p[1])))
+    return set_err(s->ctx, FRG_ERR_INVALID_ARG, "eps_rho, eps_p must be > 0");
+  s->trace_id = id;
+  s->trace_params[0] = id ? p[0] : 0.0;
+  s->trace_params[1] = id ? p[1] : 0.0;
+  if (s->dim == 1) {
+    s->L1.phys.trace_hook = id;
+    s->L1.phys.trace_p0 = s->trace_params[0];
+    s->L1.phys.trace_p1 = s->trace_params[1];
+  }
+  return FRG_OK;
+}
+
 // preprocess_state slot: the work state's buffer is allocated on selection
 static int set_pre_hook(frg_solve* s, int id, const double* params, int nparams) {
   if (id != 0 && id != kHookPrePositivity)
@@ -380,6 +407,15 @@ int frg_solve_set_hook(frg_solve* s, int slot, int id, const double* params, int
     const int rc = set_pre_hook(s, id, params, nparams);
     if (rc) return rc;
     if (s->graph) {  // captured step graphs do not contain the hook
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+    }
+    return FRG_OK;
+  }
+  if (slot == FRG_HOOK_EXTRAPOLATE_INTERFACE) {
+    const int rc = set_trace_hook(s, id, params, nparams);
+    if (rc) return rc;
+    if (s->graph) {  // captured step graphs bake the kernel parameters in
       cudaGraphExecDestroy(s->graph);
       s->graph = nullptr;
     }
@@ -430,15 +466,16 @@ int frg_apply_post_step(frg_solve* s) {
 }
 
 int frg_solve_hook_calls(frg_solve* s, int64_t* counts, int n) {
-  if (!s || !counts || n < 1 || n > 3) return FRG_ERR_INVALID_ARG;
+  if (!s || !counts || n < 1 || n > 4) return FRG_ERR_INVALID_ARG;
   cudaSetDevice(s->ctx->device);
-  long long c[3] = {0, 0, 0};
+  long long c[4] = {0, 0, 0, 0};
   cudaError_t e = cudaMemcpyAsync(c, s->sc->hook_calls, sizeof(c), cudaMemcpyDeviceToHost, s->ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
   if (e != cudaSuccess) return cuda_err(s->ctx, e, "hook counters");
   for (int i = 0; i < n; ++i) counts[i] = c[i];
-  // the numerical-flux override runs inline in every interface pass: no launch of its own to count
+  // the flux and trace overrides run inline in every interface pass: no launch of their own to count
   if (n > FRG_HOOK_NUMERICAL_FLUX) counts[FRG_HOOK_NUMERICAL_FLUX] = -1;
+  if (n > FRG_HOOK_EXTRAPOLATE_INTERFACE) counts[FRG_HOOK_EXTRAPOLATE_INTERFACE] = -1;
   return FRG_OK;
 }
 

@@ -35,6 +35,7 @@ struct OpsT {
   double Vinv[NP][NP];
   double lL[NP], lR[NP], lLD[NP], lRD[NP], gL[NP], gR[NP];
   double xi[NP];
+  double w[NP];  // quadrature weights (element means)
 };
 
 // Host copy of all tables for one (p, points) pair (NP <= kMaxNp).
@@ -107,7 +108,7 @@ struct DevScalars {
   long long residual_evals;
   // launches of each hook slot's kernel that passed their gate (indexed by
   // FRG_HOOK_*); counted on the device and never overwritten from the host
-  long long hook_calls[3];
+  long long hook_calls[4];
 };
 
 enum : int { kRunning = 0, kFinished = 3 };
@@ -119,6 +120,8 @@ enum : int {
   kHookFluxRusanov = 2,      // numerical_flux: Rusanov, dissipation scaled by a parameter
   kHookFluxHLLC = 3,         // numerical_flux: HLLC
   kHookPrePositivity = 4,    // preprocess_state: Zhang-Shu scaling of the work state
+  kHookTraceMean = 5,        // extrapolate_interface: traces pulled toward the element mean
+  kHookTracePositivity = 6,  // extrapolate_interface: Zhang-Shu scaling of the traces
 };
 
 // Stage kernel launch parameters (shared by the 1D and 2D kernels).
@@ -151,6 +154,10 @@ struct Phys {
   // 1D interface flux: dissipation scale of the Rusanov flux (1 except under
   // a numerical_flux_method override that scales it)
   double flux_alpha;
+  // 1D interface traces: extrapolate_interface override (kHookTrace*, 0:
+  // the Lagrange traces) and its two parameters
+  double trace_p0, trace_p1;
+  int trace_hook;
   int p, pm;  // p, max(p,1)
 };
 

@@ -54,6 +54,7 @@ OpsT<NP> make_ops(const HostOps& h) {
     o.gL[i] = h.gLxi[i];
     o.gR[i] = h.gRxi[i];
     o.xi[i] = h.xi[i];
+    o.w[i] = h.w[i];
   }
   return o;
 }

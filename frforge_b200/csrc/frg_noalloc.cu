@@ -18,8 +18,7 @@
 //   - every GPU that loads the library holds the array (about 4.2 MB) until
 //     the process exits;
 //   - the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (device-specific set-up); make that first call
-//     before any stream capture on that device;
+//     cudaGetSymbolAddress (device-specific set-up);
 //   - all calls share the array and it keeps the last call's contents: every
 //     call rewrites what it reads, but calls that overlap on the GPU (two
 //     streams, or two host threads) race on it and must be serialised by the
@@ -173,6 +172,9 @@ extern "C" int frg_residual2d_noalloc(const frg_solve_desc* d, const double* u, 
   }
   Phys& P = L.phys;
   P.flux_alpha = 1.0;
+  P.trace_hook = 0;
+  P.trace_p0 = 0.0;
+  P.trace_p1 = 0.0;
   P.gamma = d->gamma;
   P.g1 = d->gamma - 1.0;
   P.c_av = d->c_av;

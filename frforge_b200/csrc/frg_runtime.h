@@ -50,6 +50,8 @@ struct frg_solve {
   int scheme_flux = 0;     // the scheme's flux (FRG_FLUX_*)
   int flux_hook_id = 0;    // numerical_flux_method override (frg_hooks.cu), 0 = none
   double flux_hook_alpha = 1.0;
+  int trace_id = 0;        // extrapolate_interface hook (frg_hooks.cu), 0 = none
+  double trace_params[2] = {0.0, 0.0};
   int pre_id = 0;          // preprocess_state hook (frg_hooks.cu), 0 = none
   double pre_params[2] = {0.0, 0.0};
   double* Uw = nullptr;    // the work state u_work of a preprocess_state hook

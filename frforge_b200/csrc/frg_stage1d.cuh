@@ -27,7 +27,8 @@ struct Smem1D {
   static constexpr int oG = oF + TX * NEQ * NP;
   static constexpr int oFace = oG + TX * NEQ * NP;  // [TX+1][8]: fhat[3], ghat[3]
   static constexpr int oSlot = oFace + (TX + 1) * 8;  // eps, J, dx
-  static constexpr int oRed = oSlot + NSLOT * 3;
+  static constexpr int oTr = oSlot + NSLOT * 3;       // [NSLOT][6]: overridden traces xi = -1, +1
+  static constexpr int oRed = oTr + NSLOT * 6;
   static constexpr int nDoubles = oRed + 32;
   static constexpr int nInts = NSLOT * 2;
   static constexpr size_t bytes = nDoubles * sizeof(double) + nInts * sizeof(int);
@@ -53,6 +54,7 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
   double* sEps = smem + S::oSlot;
   double* sJ = sEps + NSLOT;
   double* sDx = sJ + NSLOT;
+  double* sTr = smem + S::oTr;
   double* sRed = smem + S::oRed;
   int* sEl = reinterpret_cast<int*>(smem + S::nDoubles);
   int* sOwn = sEl + NSLOT;
@@ -108,6 +110,41 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
   }
   __syncthreads();
 
+  // extrapolate_interface override (residual!, Residual.jl:175): both traces
+  // of every staged element, for the numerical fluxes; the BR0 terms keep
+  // the Lagrange traces, as apply_dissipation_br0! computes its own
+  const bool trh = !prime && P.trace_hook != 0;
+  if (trh) {
+    double ws = 0.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) ws += ops.w[i];
+    for (int s = tid; s < NSLOT; s += nthr) {
+      if (sEl[s] < 0) continue;
+      double m[3], tl[3], tr[3];
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) {
+        double a = 0.0, l = 0.0, r = 0.0;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+          const double v = sU[(s * NEQ + c) * NP + i];
+          a += ops.w[i] * v;
+          l += ops.lL[i] * v;
+          r += ops.lR[i] * v;
+        }
+        m[c] = a / ws;
+        tl[c] = l;
+        tr[c] = r;
+      }
+      trace_override1(P.trace_hook, P.trace_p0, P.trace_p1, P.g1, m, tl, tr);
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) {
+        sTr[s * 6 + c] = tl[c];
+        sTr[s * 6 + 3 + c] = tr[c];
+      }
+    }
+    __syncthreads();
+  }
+
   if (!prime) {
     // P1: physical flux at own solution points
     for (int idx = tid; idx < TX * NP; idx += nthr) {
@@ -157,9 +194,16 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
           gB[c] = sg;
         }
       }
+      // the numerical flux's traces: the override's, or the Lagrange ones
+      double fA[3], fB[3];
+#pragma unroll
+      for (int c = 0; c < NEQ; ++c) {
+        fA[c] = (trh && eA >= 0) ? sTr[sA * 6 + 3 + c] : uA[c];
+        fB[c] = (trh && eB >= 0) ? sTr[sB * 6 + c] : uB[c];
+      }
       double fh[3], gh[3] = {0.0, 0.0, 0.0};
       if (eA >= 0 && eB >= 0) {
-        iflux1<FLUX>(P.gamma, P.g1, uA, uB, fh, P.flux_alpha);
+        iflux1<FLUX>(P.gamma, P.g1, fA, fB, fh, P.flux_alpha);
         if (kBR0) {
           const double sa = sEps[sA] / sJ[sA], sb = sEps[sB] / sJ[sB];
           const double tau = br0_tau(sEps[sA], sEps[sB], sDx[sA], sDx[sB], P.p);
@@ -168,8 +212,8 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
         }
       } else if (eB >= 0) {  // domain left end (Residual.jl:63-89)
         double ug[3];
-        exterior1(M.bc[0], uB, -1.0, ug);
-        iflux1<FLUX>(P.gamma, P.g1, ug, uB, fh, P.flux_alpha);
+        exterior1(M.bc[0], fB, -1.0, ug);
+        iflux1<FLUX>(P.gamma, P.g1, ug, fB, fh, P.flux_alpha);
         if (kBR0) {
           const double sb = sEps[sB] / sJ[sB];
 #pragma unroll
@@ -177,8 +221,8 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
         }
       } else {  // domain right end (Residual.jl:91-112)
         double ug[3];
-        exterior1(M.bc[1], uA, 1.0, ug);
-        iflux1<FLUX>(P.gamma, P.g1, uA, ug, fh, P.flux_alpha);
+        exterior1(M.bc[1], fA, 1.0, ug);
+        iflux1<FLUX>(P.gamma, P.g1, fA, ug, fh, P.flux_alpha);
         if (kBR0) {
           const double sa = sEps[sA] / sJ[sA];
 #pragma unroll

@@ -775,10 +775,13 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
           }
         }
       }
-      const int any_du = __syncthreads_or(chk_du != chk_du);
-      const int any_u = __syncthreads_or(chk_u != chk_u);
-      if (tid == 0 && (any_du || any_u)) {
-        if (B.sc)
+      // one barrier (P6 reads what P5 wrote) that also votes on non-finite
+      // values; only a tile with one tells the residual and the state apart
+      const bool bad_du = chk_du != chk_du, bad_u = chk_u != chk_u;
+      if (__syncthreads_or(bad_du || bad_u)) {
+        const int any_du = __syncthreads_or(bad_du);
+        const int any_u = __syncthreads_or(bad_u);
+        if (tid == 0 && B.sc)
           atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
       }
     }

@@ -214,9 +214,9 @@ class GpuSolve:
     def hook_calls(self) -> dict:
         """Device-counted invocations per hook slot since the solve was made
         (the HookProbeMethod counters of test/test_capturing.jl); the inline
-        numerical_flux_method slot reports None."""
-        c = (C.c_int64 * 3)()
-        self._chk(L.load().frg_solve_hook_calls(self.handle, c, 3), "frg_solve_hook_calls")
+        numerical_flux_method and extrapolate_interface slots report None."""
+        c = (C.c_int64 * len(L.HOOK_SLOT))()
+        self._chk(L.load().frg_solve_hook_calls(self.handle, c, len(c)), "frg_solve_hook_calls")
         return {name: (None if c[i] < 0 else int(c[i])) for name, i in L.HOOK_SLOT.items()}
 
     def close(self):

@@ -239,6 +239,96 @@ class FluxOverridePersson(PerssonAVMethod):
         return p
 
 
+def _root01(a, b, c):
+    """Smallest root in [0, 1] of a t^2 + b t + c (c > 0 >= a + b + c), the
+    stable quadratic formula of the device limiter."""
+    import math
+
+    if abs(a) < 1e-300:
+        return min(max(-c / b, 0.0), 1.0) if b != 0.0 else 0.0
+    disc = max(b * b - 4.0 * a * c, 0.0)
+    q = -0.5 * (b + math.copysign(math.sqrt(disc), b))
+    r1, r2 = q / a, (c / q if q != 0.0 else 2.0)
+    t = 1.0
+    for r in (r1, r2):
+        if 0.0 <= r <= 1.0:
+            t = min(t, r)
+    return t
+
+
+class TraceOverridePersson(PerssonAVMethod):
+    """Persson AV whose extrapolate_interface! (Interfaces.jl:49-71, "Override
+    for hybrid reconstruction") replaces the Lagrange traces that the 1D
+    interface fluxes use: kind="toward_mean" pulls each element's two traces
+    toward its mean, ubar + theta (ell . u - ubar) (theta = 1: the default
+    traces, theta = 0: first order); kind="positivity" applies the
+    Zhang-Shu scaling to them (density >= eps_rho, then pressure >= eps_p).
+    A src/methods-style plugin naming the device implementation of the hook
+    ("traces_toward_mean" / "traces_positivity_zhang_shu", frg_hooks.cu).
+    As in the reference, only the 1D residual calls it, and the BR0
+    dissipation keeps the Lagrange traces."""
+
+    def __init__(self, kind="toward_mean", theta=1.0, eps_rho=1e-13, eps_p=1e-13, kappa=4.0, s0_factor=-4.0,
+                 c_av=0.1, av_form="conservative_br0"):
+        super().__init__(kappa, s0_factor, c_av, av_form)
+        if kind not in ("toward_mean", "positivity"):
+            raise ValueError("kind must be 'toward_mean' or 'positivity'")
+        self.kind, self.theta = kind, float(theta)
+        self.eps_rho, self.eps_p = float(eps_rho), float(eps_p)
+        self.gpu_hooks = {"extrapolate_interface": (
+            ("traces_toward_mean", (self.theta,)) if kind == "toward_mean"
+            else ("traces_positivity_zhang_shu", (self.eps_rho, self.eps_p)))}
+
+    def element_traces(self, ue, w, lL, lR, gamma=1.4):
+        """Host restatement for one element: ue[j, c] (1D Euler, conserved),
+        quadrature weights w and Lagrange rows lL, lR -> (trace at xi = -1,
+        trace at xi = +1)."""
+        import numpy as np
+
+        ue, w = np.asarray(ue, dtype=np.float64), np.asarray(w, dtype=np.float64)
+        m = (w @ ue) / w.sum()
+        tl, tr = np.asarray(lL) @ ue, np.asarray(lR) @ ue
+        if self.kind == "toward_mean":
+            return m + self.theta * (tl - m), m + self.theta * (tr - m)
+        g1 = gamma - 1.0
+
+        def pres(U):
+            return g1 * (U[2] - 0.5 * U[1] * U[1] / U[0])
+
+        if not (m[0] > self.eps_rho) or not (pres(m) > self.eps_p):
+            return tl, tr
+        rmin = min(tl[0], tr[0])
+        if rmin < self.eps_rho:
+            th = (m[0] - self.eps_rho) / (m[0] - rmin)
+            tl[0], tr[0] = m[0] + th * (tl[0] - m[0]), m[0] + th * (tr[0] - m[0])
+        theta = 1.0
+        for U in (tl, tr):
+            if pres(U) >= self.eps_p:
+                continue
+            d = U - m
+            a = g1 * (d[2] * d[0] - 0.5 * d[1] * d[1])
+            b = g1 * (m[2] * d[0] + m[0] * d[2] - m[1] * d[1]) - self.eps_p * d[0]
+            c = m[0] * (pres(m) - self.eps_p)
+            theta = min(theta, _root01(a, b, c))
+        if theta < 1.0:
+            tl, tr = m + theta * (tl - m), m + theta * (tr - m)
+        return tl, tr
+
+    def extrapolate_interface_(self, traces, u_work, state, eq):
+        """Host restatement over a 1D state: traces = (uL[e, c], uR[e, c])."""
+        uL, uR = traces
+        ops = state.ops
+        for e in range(u_work.shape[1]):
+            uL[e], uR[e] = self.element_traces(u_work[:, e, :], ops.w, ops.l_L, ops.l_R, eq.gamma)
+        return traces
+
+    def method_params(self):
+        p = super().method_params()
+        p.update({"method": "persson_av_trace_override", "kind": self.kind, "theta": self.theta,
+                  "eps_rho": self.eps_rho, "eps_p": self.eps_p})
+        return p
+
+
 _GPU_CLASSES = (ScaledPerssonMethod, PerssonAVMethod, NullCapturing)
 
 # Method registry (Interfaces.jl:118-135, src/methods/Registry.jl:14-53)
@@ -249,6 +339,7 @@ METHOD_REGISTRY: Dict[str, Callable[..., AbstractCapturingMethod]] = {
     "persson_av_positive": lambda **kw: PositivityPreservingPersson(**kw),
     "persson_av_flux_override": lambda **kw: FluxOverridePersson(**kw),
     "persson_av_preprocess_positive": lambda **kw: PositivityPreprocessPersson(**kw),
+    "persson_av_trace_override": lambda **kw: TraceOverridePersson(**kw),
 }
 
 

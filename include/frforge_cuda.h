@@ -242,9 +242,9 @@ int frg_autotune_table_size(void);
    cudaStream_t (NULL: legacy default stream).  All scratch lives in one
    fixed __device__ array (at most FRG_NOALLOC_MAX_ELEMENTS elements,
    FRG_NOALLOC_MAX_SIDE per side; larger meshes return FRG_ERR_INVALID_ARG).
-   The first call on a device resolves that array's address: make it before
-   any stream capture.  Calls share the array: calls that overlap on the GPU
-   race and must be serialised by the caller.  Returns after enqueueing. */
+   The first call on a device resolves that array's address
+   (cudaGetSymbolAddress).  Calls share the array: calls that overlap on the
+   GPU race and must be serialised by the caller.  Returns after enqueueing. */
 int frg_residual2d_noalloc(const frg_solve_desc* desc, const double* u, double* du,
                            double t, void* stream);
 
@@ -479,7 +479,10 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
    ssp_rk3_step!, SSP_RK3.jl:162); numerical_flux_method (the flux of every
    1D interface, boundary interfaces included, as _resolve_flux,
    src/fr/Residual.jl:9-15; the 2D residual ignores it, as the reference's
-   does); preprocess_state (the state the residual is evaluated on).
+   does); preprocess_state (the state the residual is evaluated on);
+   extrapolate_interface (the element traces the 1D interface fluxes use, as
+   extrapolate_interface! in residual!, Residual.jl:175; the 2D residual
+   never calls it, and a 2D solve ignores the slot).
    Implementations:
      "positivity_zhang_shu"  post_step: the positivity-preserving scaling of
         Zhang & Shu (J. Comput. Phys. 229, 2010) toward the element mean,
@@ -495,11 +498,25 @@ int frg_server_submit_ic(frg_server* s, const frg_solve_desc* desc, const frg_ic
         the stage state (preprocess_state!, Interfaces.jl:41-46, called first
         in residual!).  Single solves only: frg_batch_start and
         frg_server_set_hook refuse it with FRG_ERR_UNSUPPORTED_HOOK.
+     "traces_toward_mean"  extrapolate_interface: each element's two traces
+        pulled toward its mean (quadrature weights), ubar + theta (t - ubar),
+        params[0] = theta in [0, 1] (default 1: the Lagrange traces, to
+        rounding; 0: first-order traces).
+     "traces_positivity_zhang_shu"  extrapolate_interface: the Zhang & Shu
+        scaling (as "positivity_zhang_shu") applied to an element's two
+        traces, density >= params[0], pressure >= params[1] (defaults 1e-13).
+        Both change only the numerical fluxes' inputs; the BR0 dissipation
+        keeps the Lagrange traces (apply_dissipation_br0!, PerssonAV.jl:249).
    Batched instances run their hooks too: set one on the slot's solve
    (frg_batch_get_solve) before frg_batch_start, or on a queued request with
    frg_server_set_hook; the batch groups instances by hook and steps them
    to the same results as a single solve. */
-enum { FRG_HOOK_POST_STEP = 0, FRG_HOOK_NUMERICAL_FLUX = 1, FRG_HOOK_PREPROCESS_STATE = 2 };
+enum {
+  FRG_HOOK_POST_STEP = 0,
+  FRG_HOOK_NUMERICAL_FLUX = 1,
+  FRG_HOOK_PREPROCESS_STATE = 2,
+  FRG_HOOK_EXTRAPOLATE_INTERFACE = 3
+};
 int frg_hook_count(void);
 int frg_hook_info(int index, const char** name, int* slot, int* id, int* nparams);
 /* FRG_ERR_UNSUPPORTED_HOOK if no implementation has that name. */
@@ -514,9 +531,10 @@ int frg_apply_post_step(frg_solve* s);
    = post-step passes run (one per completed step, plus each
    frg_apply_post_step), counts[FRG_HOOK_PREPROCESS_STATE] = work states made
    (one per residual evaluation: stage, frg_residual, frg_sense).  The flux
-   override runs inline in every interface pass, with no launch of its own:
-   counts[FRG_HOOK_NUMERICAL_FLUX] = -1 (frg_solve_info.residual_evals counts
-   the residuals that used it).  n: entries to fill, 1..3. */
+   and trace overrides run inline in every interface pass, with no launch of
+   their own: counts[FRG_HOOK_NUMERICAL_FLUX] =
+   counts[FRG_HOOK_EXTRAPOLATE_INTERFACE] = -1 (frg_solve_info.residual_evals
+   counts the residuals that used them).  n: entries to fill, 1..4. */
 int frg_solve_hook_calls(frg_solve* s, int64_t* counts, int n);
 /* Select hook `id` of `slot` for a request that is still queued (id 0
    removes it); applied to the request's solve at admission.  FRG_ERR_STATE

@@ -371,6 +371,8 @@ struct orc_solver {
   double kappa, s0_factor, eps_floor, c_av;
   int flux_override;  /* numerical_flux_method override (1D): -1 none, else ORC_FLUX_* */
   double flux_alpha;  /* its Rusanov dissipation scale */
+  int trace_override; /* extrapolate_interface override (1D): 0 none, ORC_TRACE_* */
+  double trace_p0, trace_p1;
   orc_bc bc[4]; /* 1D: [0]=left [1]=right; 2D: left right bottom top */
   double t;
   /* 1D mesh */
@@ -447,6 +449,9 @@ orc_solver* orc_create_1d(int p, int points, int nel, double xl, double xr,
   s->flux = flux;
   s->flux_override = -1;
   s->flux_alpha = 1.0;
+  s->trace_override = 0;
+  s->trace_p0 = 0.0;
+  s->trace_p1 = 0.0;
   s->time_scheme = time_scheme;
   s->method = method;
   s->av_form = av_form;
@@ -700,6 +705,9 @@ orc_solver* orc_create_2d(int p, int points, int nx, int ny, double xl,
   s->flux = flux;
   s->flux_override = -1;
   s->flux_alpha = 1.0;
+  s->trace_override = 0;
+  s->trace_p0 = 0.0;
+  s->trace_p1 = 0.0;
   s->time_scheme = time_scheme;
   s->method = method;
   s->av_form = av_form;
@@ -1342,6 +1350,77 @@ static void local_dd_1d(orc_solver* s, double* du, const double* uw) {
   }
 }
 
+/* smallest root in [0, 1] of a t^2 + b t + c with c > 0 >= a + b + c, the
+   stable quadratic formula (the pressure condition of the Zhang & Shu
+   positivity-preserving scaling, J. Comput. Phys. 229 (2010) 8918-8934) */
+static double root01(double a, double b, double c) {
+  if (fabs(a) < 1e-300) return b != 0.0 ? fmin(fmax(-c / b, 0.0), 1.0) : 0.0;
+  double disc = fmax(b * b - 4.0 * a * c, 0.0);
+  double q = -0.5 * (b + copysign(sqrt(disc), b));
+  double r1 = q / a, r2 = q != 0.0 ? c / q : 2.0;
+  double t = 1.0;
+  if (r1 >= 0.0 && r1 <= 1.0) t = fmin(t, r1);
+  if (r2 >= 0.0 && r2 <= 1.0) t = fmin(t, r2);
+  return t;
+}
+
+/* A method's extrapolate_interface! override (Interfaces.jl:49-71 is the
+   default, "Override for hybrid reconstruction") applied to one element's
+   traces tl (xi = -1) and tr (xi = +1) given its mean m: ORC_TRACE_MEAN
+   pulls them toward the mean by p0 in [0, 1]; ORC_TRACE_POSITIVITY scales
+   them toward it until density >= p0 and then pressure >= p1 (Zhang & Shu),
+   an element with an inadmissible mean left as it is. */
+static void trace_override_1d(const orc_solver* s, const double* m, double* tl, double* tr) {
+  const double g1 = s->gamma - 1.0;
+  if (s->trace_override == ORC_TRACE_MEAN) {
+    for (int c = 0; c < 3; ++c) {
+      tl[c] = m[c] + s->trace_p0 * (tl[c] - m[c]);
+      tr[c] = m[c] + s->trace_p0 * (tr[c] - m[c]);
+    }
+    return;
+  }
+  if (s->trace_override != ORC_TRACE_POSITIVITY) return;
+  const double er = s->trace_p0, ep = s->trace_p1;
+  const double pbar = g1 * (m[2] - 0.5 * m[1] * m[1] / m[0]);
+  if (!(m[0] > er) || !(pbar > ep)) return;
+  const double rmin = fmin(tl[0], tr[0]);
+  if (rmin < er) {
+    const double th = (m[0] - er) / (m[0] - rmin);
+    tl[0] = m[0] + th * (tl[0] - m[0]);
+    tr[0] = m[0] + th * (tr[0] - m[0]);
+  }
+  double theta = 1.0;
+  for (int side = 0; side < 2; ++side) {
+    const double* U = side == 0 ? tl : tr;
+    const double pk = g1 * (U[2] - 0.5 * U[1] * U[1] / U[0]);
+    if (pk >= ep) continue;
+    const double d0 = U[0] - m[0], d1 = U[1] - m[1], d2 = U[2] - m[2];
+    const double a = g1 * (d2 * d0 - 0.5 * d1 * d1);
+    const double b = g1 * (m[2] * d0 + m[0] * d2 - m[1] * d1) - ep * d0;
+    const double cc = m[0] * (pbar - ep);
+    theta = fmin(theta, root01(a, b, cc));
+  }
+  if (theta < 1.0)
+    for (int c = 0; c < 3; ++c) {
+      tl[c] = m[c] + theta * (tl[c] - m[c]);
+      tr[c] = m[c] + theta * (tr[c] - m[c]);
+    }
+}
+
+void orc_set_trace_override(orc_solver* s, int kind, double p0, double p1) {
+  s->trace_override = kind;
+  s->trace_p0 = p0;
+  s->trace_p1 = p1;
+}
+
+/* the 1D traces the last residual's interface fluxes used, [nel, 3] each
+   (Julia layout: trL[e + nel*c]) */
+void orc_get_traces_1d(const orc_solver* s, double* trL, double* trR) {
+  const size_t n = (size_t)s->nel * 3;
+  memcpy(trL, s->trL, n * sizeof(double));
+  memcpy(trR, s->trR, n * sizeof(double));
+}
+
 /* residual! 1D, src/fr/Residual.jl:161-214 (interface fluxes :24-115,
    default extrapolate_interface! src/capturing/Interfaces.jl:49-71) */
 static void residual_1d(orc_solver* s, double* du) {
@@ -1360,6 +1439,25 @@ static void residual_1d(orc_solver* s, double* du) {
       s->trL[e + nel * c] = sL;
       s->trR[e + nel * c] = sR;
     }
+  if (s->trace_override) {
+    double wsum = 0.0;
+    for (int j = 0; j < np; ++j) wsum += s->ops.w[j];
+    for (int e = 0; e < nel; ++e) {
+      double m[3], tl[3], tr[3];
+      for (int c = 0; c < neq; ++c) {
+        double a = 0.0;
+        for (int j = 0; j < np; ++j) a += s->ops.w[j] * uw[c * cs + (size_t)np * e + j];
+        m[c] = a / wsum;
+        tl[c] = s->trL[e + nel * c];
+        tr[c] = s->trR[e + nel * c];
+      }
+      trace_override_1d(s, m, tl, tr);
+      for (int c = 0; c < neq; ++c) {
+        s->trL[e + nel * c] = tl[c];
+        s->trR[e + nel * c] = tr[c];
+      }
+    }
+  }
   double um[3], up[3], ft[3];
   for (int e = 0; e < nel - 1; ++e) {
     for (int c = 0; c < neq; ++c) {

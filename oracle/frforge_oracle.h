@@ -132,6 +132,14 @@ double orc_l2_error_density_wave_1d(const orc_solver* s, double t);
 /* numerical_flux_method override of the 1D residual: kind -1 none,
    ORC_FLUX_RUSANOV (dissipation scaled by alpha) or ORC_FLUX_HLLC */
 void orc_set_flux_override(orc_solver* s, int kind, double alpha);
+/* A 1D method's extrapolate_interface! override: ORC_TRACE_NONE (0) clears
+   it; ORC_TRACE_MEAN (p0 = theta) pulls each element's traces toward its
+   mean; ORC_TRACE_POSITIVITY (p0 = eps_rho, p1 = eps_p) scales them
+   (Zhang-Shu).  Only the interface fluxes use the traces. */
+enum { ORC_TRACE_NONE = 0, ORC_TRACE_MEAN = 1, ORC_TRACE_POSITIVITY = 2 };
+void orc_set_trace_override(orc_solver* s, int kind, double p0, double p1);
+/* 1D: the traces the last orc_residual's interface fluxes used, [nel,3] each */
+void orc_get_traces_1d(const orc_solver* s, double* trL, double* trR);
 
 /* single-interface fluxes (unit checks) */
 void orc_hllc_1d(double gamma, const double* uL, const double* uR, double* out);

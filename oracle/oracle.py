@@ -111,6 +111,8 @@ def lib():
         L.orc_physical_coords.argtypes = [C.c_void_p, dp, dp]
         L.orc_set_threads.argtypes = [ip]
         L.orc_set_flux_override.argtypes = [C.c_void_p, ip, C.c_double]
+        L.orc_set_trace_override.argtypes = [C.c_void_p, ip, C.c_double, C.c_double]
+        L.orc_get_traces_1d.argtypes = [C.c_void_p, dp, dp]
         L.orc_residual.argtypes = [C.c_void_p, dp]
         L.orc_sense.argtypes = [C.c_void_p, dp]
         L.orc_compute_dt.restype = C.c_double
@@ -263,6 +265,19 @@ class OracleSolver:
         flux), "rusanov" (dissipation scaled by alpha) or "hllc"."""
         k = -1 if kind is None else {"rusanov": 0, "hllc": 1}[kind]
         lib().orc_set_flux_override(self._h, k, float(alpha))
+
+    def set_trace_override(self, kind=None, p0: float = 1.0, p1: float = 1e-13) -> None:
+        """A 1D method's extrapolate_interface! override: None (the Lagrange
+        traces), "toward_mean" (p0 = theta) or "positivity" (p0 = eps_rho,
+        p1 = eps_p)."""
+        k = 0 if kind is None else {"toward_mean": 1, "positivity": 2}[kind]
+        lib().orc_set_trace_override(self._h, k, float(p0), float(p1))
+
+    def traces_1d(self):
+        """(uL, uR) [nel, 3]: the traces the last residual's fluxes used."""
+        tl, tr = np.zeros(self.nel * 3), np.zeros(self.nel * 3)
+        lib().orc_get_traces_1d(self._h, _dp(tl), _dp(tr))
+        return tl.reshape(self.nel, 3, order="F"), tr.reshape(self.nel, 3, order="F")
 
     def residual(self) -> np.ndarray:
         du = np.zeros(self.ndof)

@@ -27,12 +27,12 @@ def _probe(state, eq, method=None):
 def test_residual_and_sense_each_make_one_work_state():
     orc, state, _ = pair_2d(p=2, nx=8, ny=6, flux="hllc", method="persson")
     s = _probe(state, F.Euler2D(1.4))
-    assert s.hook_calls() == {"post_step": 0, "numerical_flux_method": None, "preprocess_state": 0}
+    assert s.hook_calls() == {"post_step": 0, "numerical_flux_method": None, "extrapolate_interface": None, "preprocess_state": 0}
     s.upload(smooth_state_2d(orc), 0.0)
     s.residual()
     assert s.hook_calls()["preprocess_state"] == 1
     s.sense()
-    assert s.hook_calls() == {"post_step": 0, "numerical_flux_method": None, "preprocess_state": 2}
+    assert s.hook_calls() == {"post_step": 0, "numerical_flux_method": None, "extrapolate_interface": None, "preprocess_state": 2}
     s.apply_post_step()
     assert s.hook_calls()["post_step"] == 1
     s.close()
@@ -54,7 +54,7 @@ def test_steps_count_one_work_state_per_stage_and_one_post_step_per_step(time, s
     assert r2["n_steps"] == 5
     s.step(1e-4)
     n = r["n_steps"] + 6
-    assert s.hook_calls() == {"post_step": n, "numerical_flux_method": None, "preprocess_state": stages * n}
+    assert s.hook_calls() == {"post_step": n, "numerical_flux_method": None, "extrapolate_interface": None, "preprocess_state": stages * n}
     s.close()
 
 
@@ -65,7 +65,7 @@ def test_1d_counts_and_the_inline_flux_override():
     s.upload(orc.u.copy(), 0.0)
     r = s.advance(0.02, cfl=0.1)
     assert r["status"] == "ok"
-    assert s.hook_calls() == {"post_step": r["n_steps"], "numerical_flux_method": None,
+    assert s.hook_calls() == {"post_step": r["n_steps"], "numerical_flux_method": None, "extrapolate_interface": None,
                               "preprocess_state": 3 * r["n_steps"]}
     assert s.info()["residual_evals"] == 3 * r["n_steps"]
     s.close()
