@@ -404,6 +404,26 @@ def run_c1(args):
     return 0
 
 
+def tune_table(F, ctx, keys, n: int = 256):
+    """Populate the persisted-tile table (frg_autotune_table_*) as a
+    deployment does before serving: for every (P, flux) key, Persson BR0 on
+    an affine mesh, the autotuner times the tile variants on an n^2 periodic
+    density wave and records the fastest.  New solves and the batched groups
+    of that key then use it.  Returns {"p<P>_<flux>": variant}."""
+    from frforge_b200.workloads import Workload2D
+
+    out = {}
+    for p, flux in keys:
+        w = Workload2D("c2", n, p, flux, "persson_av", 0.1, True, 0.1, 4)
+        st, m = w.build(F)
+        s = F.GpuSolve(st, F.Euler2D(1.4), m, ctx=ctx)
+        s.upload(st.u, 0.0)
+        best, _ = s.autotune(reps=3)
+        out[f"p{p}_{flux}"] = int(best)
+        s.close()
+    return out
+
+
 def run_batched(args):
     """64 independent mixed solves (frforge_b200.workloads.c4_instances), each
     200 SSP-RK3 steps: solves/s of the batched engine (frg_batch_*) against
@@ -435,6 +455,9 @@ def run_batched(args):
     steps = args.batch_steps
     cfl = inst[0].cfl
     esz = u_in.element_size()
+    # tile table for both arms (solves read it at creation, batched groups
+    # at grouping), outside the timed region
+    tiles = {} if args.no_tune else tune_table(F, ctx, sorted({(w.p, w.flux) for w in inst}))
 
     # sequential arm: one GpuSolve per instance, run one after the other
     solves = [F.GpuSolve(st, eq, m, ctx=ctx) for st, m in built]
@@ -509,7 +532,8 @@ def run_batched(args):
                                    "HLLC/Rusanov, Persson AV c_av=0.1*U[0.5,2], half periodic density "
                                    "waves, half transmissive four-quadrant ICs, 200 SSP-RK3 steps, CFL 0.1",
                        "elements": int(sum(w.n * w.n for w in inst)), "dof": int(offs[-1]),
-                       "groups": ngroups, "reps": reps},
+                       "groups": ngroups, "reps": reps,
+                       "tile_table": tiles or "empty (default tiles)"},
             "sequential": {"value": len(inst) / (t_seq * 1e-3), "unit": "solves/s", "ms": t_seq},
             "speedup_vs_sequential": t_seq / t_bat,
             "ideal_speedup": t_seq / t_ideal,
@@ -574,6 +598,9 @@ def run_served(args):
     torch.cuda.set_device(local)
     ctx = F.Context(local)
     trace = served_trace(count=args.served_requests)
+    # tile table for both arms (2D affine keys), outside the timed region
+    tiles = {} if args.no_tune else tune_table(
+        F, ctx, sorted({(r.p, r.flux) for r in trace if r.dim == 2 and not r.wavy}))
     # mesh and scheme only: both arms evaluate each request's IC on the device
     built = [req.build(F, fill=False) for req in trace]
     ics = [req.ic() for req in trace]
@@ -648,7 +675,8 @@ def run_served(args):
                                "(1/4 wavy, amplitude 0.05), P~U{1..5}, HLLC/Rusanov, density wave or "
                                "Riemann IC (jumps x0.25), periodic, t_final~U[0.05,0.25], Persson AV, "
                                "SSP-RK3, CFL 0.1",
-                   "requests": len(trace), "slots": 64, "steps_per_pump": 8},
+                   "requests": len(trace), "slots": 64, "steps_per_pump": 8,
+                   "tile_table": tiles or "empty (default tiles)"},
         "latency_s": {"p50": float(np.percentile(lat_s, 50)), "p99": float(np.percentile(lat_s, 99)),
                       "max": float(lat_s.max())},
         "sequential": {"value": len(trace) / span_q, "unit": "solves/s",
@@ -705,6 +733,8 @@ def main():
                     help="--ncu-target: capturing method (default: the workload's, Persson AV)")
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--batch-reps", type=int, default=3)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="--workload batched/served: leave the autotune table empty (default tiles)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
