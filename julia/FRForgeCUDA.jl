@@ -21,7 +21,9 @@
 #     that varies is refused), and GhostStateBC only where the case declares
 #     its x-split form through `ghost_xsplit` (the double-Mach shape);
 #   * NullCapturing, PerssonAVMethod, ScaledPerssonMethod, and any method
-#     that declares `gpu_method_form`; other hook overrides are refused.
+#     that declares `gpu_method_form`, with `gpu_hooks` naming the library's
+#     device implementations of the hooks it overrides (selected on the
+#     solve by `gpu`); other hook overrides are refused.
 #
 # The structs below mirror the C structs field for field (same names, same
 # order); tests/test_julia_layout.py computes their layout under the C rules
@@ -206,6 +208,33 @@ gpu_method_form(m::ScaledPerssonMethod) = gpu_method_form(m.inner)
 gpu_method_form(m::AbstractCapturingMethod) = throw(ArgumentError(
     "$(typeof(m)) overrides hooks with no GPU implementation (FRG_ERR_UNSUPPORTED_HOOK)"))
 
+"""
+    gpu_hooks(method) -> Vector{Tuple{String, Vector{Float64}}}
+
+The device implementations a src/methods plugin selects for the hooks it
+overrides, by registry name with their parameters (frg_hook_info lists
+them: "positivity_zhang_shu" for post_step!, "flux_rusanov" / "flux_hllc"
+for numerical_flux_method, "preprocess_positivity_zhang_shu" for
+preprocess_state!, "traces_toward_mean" / "traces_positivity_zhang_shu"
+for extrapolate_interface!).  The built-in methods select none.  A plugin
+adds a `gpu_method_form` method (its descriptor fields, usually those of the
+Persson method it wraps) and a `gpu_hooks` method naming its hooks'
+implementations; `gpu(...)` selects them on the solve.
+"""
+gpu_hooks(::AbstractCapturingMethod) = Tuple{String, Vector{Float64}}[]
+gpu_hooks(m::ScaledPerssonMethod) = gpu_hooks(m.inner)
+
+function select_hooks!(g, method)
+    for (name, params) in gpu_hooks(method)
+        sl, id = Ref{Cint}(), Ref{Cint}()
+        check(ccall((:frg_hook_lookup, LIB), Cint, (Cstring, Ref{Cint}, Ref{Cint}), name, sl, id), g.ctx)
+        p = Vector{Float64}(params)
+        check(ccall((:frg_solve_set_hook, LIB), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{Float64}, Cint),
+                    g.solve, sl[], id[], isempty(p) ? Ptr{Float64}(C_NULL) : pointer(p), length(p)), g.ctx)
+    end
+    return g
+end
+
 # ------------------------------------------------------------------- solves
 
 mutable struct GPUSolutionState
@@ -278,7 +307,7 @@ function gpu(state::SolutionState2D, eq::Euler2D, method::AbstractCapturingMetho
                             pointer(yv), bcs, solid, geometry, 0.0, metrics,
                             Base.unsafe_convert(Ptr{FrgOperators}, ops), gpu_method_form(method)...))
     push!(keep, desc)
-    return create(desc, state, keep, device)
+    return select_hooks!(create(desc, state, keep, device), method)
 end
 
 """gpu(state::SolutionState, eq::Euler1D, method; device = 0)"""
@@ -295,7 +324,7 @@ function gpu(state::SolutionState, eq::Euler1D, method::AbstractCapturingMethod;
                             0.0, Ptr{FrgMetrics2D}(C_NULL), Base.unsafe_convert(Ptr{FrgOperators}, ops),
                             gpu_method_form(method)...))
     push!(keep, desc)
-    return create(desc, state, keep, device)
+    return select_hooks!(create(desc, state, keep, device), method)
 end
 
 function upload!(g::GPUSolutionState)
