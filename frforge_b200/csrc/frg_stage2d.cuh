@@ -71,6 +71,22 @@ struct Tile2D<6> {
 
 constexpr int odd_up(int n) { return (n % 2) ? n : n + 1; }
 
+// Element stride (doubles) of a staged element, NEQ * NP2 padded so that the
+// warps' 8-byte shared loads of P1-P5 spread over the 16 bank pairs: picked
+// per tile shape with a model of the phases' address patterns (wavefronts =
+// most distinct words on one bank pair) -- e.g. 3.07 -> 2.60 wavefronts per
+// load on the 4x4 P=3 tile, 2.68 -> 2.38 on the 8x2 one; on a B200 the 512^2
+// P=3 stage kernel gained 5.7 % (64.7 -> 68.4 G DOF-stage/s), with the
+// vertical face order below.
+constexpr int stage_es(int np, int tx, int ty) {
+  return np == 2 ? (tx == 16 ? (ty == 8 ? 17 : 19) : 23)  // 16x8: 19 would not fit two CTAs
+       : np == 3 ? 41
+       : np == 4 ? ((tx == 8 && ty == 4) ? 65 : 67)
+       : np == 5 ? 105
+       : np == 6 ? (tx == 6 ? 151 : 153)
+       : odd_up(4 * np * np);
+}
+
 // Shared-memory layout.  U0S: stage the step-start state u0 in shared memory
 // (copied with the tile); otherwise the epilogue reads it from global memory.
 template <int NP, int TX, int TY, bool U0S = true, int MINB = 2, int NTHR = 256>
@@ -79,7 +95,7 @@ struct Smem2D {
   static constexpr int NEQ = 4, NP2 = NP * NP;
   static constexpr int BX = TX + 2, BY = TY + 2, NSLOT = BX * BY, NOWN = TX * TY;
   static constexpr int NFV = (TX + 1) * TY, NFH = TX * (TY + 1);
-  static constexpr int ES = odd_up(NEQ * NP2);  // element stride (doubles)
+  static constexpr int ES = stage_es(NP, TX, TY);  // element stride (doubles)
   static constexpr int FS = odd_up(NP * 8);     // face stride: NP points x (fhat[4], ghat[4])
   // one tile buffer (doubles): u_s of tile + halo, u0 of the tile, per-slot
   // mesh values [6][NSLOT] = eps, Jx, Jy, 1/Jx, 1/Jy, h_char
@@ -340,10 +356,21 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
       const bool vert = idx < NFV * NP;
       const int id2 = vert ? idx : idx - NFV * NP;
       int f, q, sA, sB;
-      if (vert) {  // lanes walk over the faces of a row
-        const int fx = id2 % (TX + 1), r = id2 / (TX + 1);
-        q = r % NP;
-        const int fy = r / NP;
+      if (vert) {
+        // lanes walk over the points of a face and then the faces of a row
+        // (P = 3, 4), or over the faces of a row (fewer bank conflicts there)
+        int fx, fy;
+        if (NP == 4 || NP == 5) {
+          q = id2 % NP;
+          const int r = id2 / NP;
+          fx = r % (TX + 1);
+          fy = r / (TX + 1);
+        } else {
+          fx = id2 % (TX + 1);
+          const int r = id2 / (TX + 1);
+          q = r % NP;
+          fy = r / NP;
+        }
         f = fy * (TX + 1) + fx;
         sA = (fy + 1) * BX + fx;
         sB = sA + 1;
