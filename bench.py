@@ -405,13 +405,18 @@ def run_c1(args):
 
 
 def tune_table(F, ctx, keys, n: int = 256):
-    """Populate the persisted-tile table (frg_autotune_table_*) as a
-    deployment does before serving: for every (P, flux) key, Persson BR0 on
-    an affine mesh, the autotuner times the tile variants on an n^2 periodic
-    density wave and records the fastest.  New solves and the batched groups
-    of that key then use it.  Returns {"p<P>_<flux>": variant}."""
+    """Fill the tile table (frg_autotune_table_*) as a deployment does before
+    serving: from the committed table measured on a B200
+    (frforge_b200/autotune_b200.json, frforge_b200.autotune.measure) when
+    present, else for every (P, flux) key, Persson BR0 on an affine mesh, by
+    timing the tile variants on an n^2 periodic density wave.  New solves and
+    the batched groups of a key then use its variant.  Returns
+    {"p<P>_<flux>": variant}."""
+    from frforge_b200 import autotune as T
     from frforge_b200.workloads import Workload2D
 
+    if T.load_default():
+        return {f"p{p}_{flux}": T.get_variant(p, flux, "br0", False) for p, flux in keys}
     out = {}
     for p, flux in keys:
         w = Workload2D("c2", n, p, flux, "persson_av", 0.1, True, 0.1, 4)

@@ -59,3 +59,41 @@ def load_default() -> bool:
         load(DEFAULT_TABLE)
         return True
     return False
+
+
+def measure(path: str = DEFAULT_TABLE, ps=(1, 2, 3, 4, 5), fluxes=("hllc", "rusanov"),
+            avs=("br0", "local_dd", "none"), reps: int = 3, ctx=None) -> dict:
+    """Build the table on this GPU and save it: for every (P, flux,
+    dissipation form) of an affine mesh, the autotuner times the tile
+    variants on a periodic density wave on a mesh that fills the device
+    (512^2 elements for P <= 3, 384^2 above) and records the fastest.
+    Returns {"p<P>_<flux>_<av>": variant}."""
+    from . import Euler2D, GpuSolve, NullCapturing, PerssonAVMethod
+    from .workloads import Workload2D
+
+    out = {}
+    for p in ps:
+        for flux in fluxes:
+            for av in avs:
+                n = 512 if p <= 3 else 384
+                w = Workload2D("c2", n, p, flux, "null" if av == "none" else "persson_av", 0.1, True, 0.1, 4)
+                st, _ = w.build(__import__(__package__))
+                m = (NullCapturing() if av == "none" else
+                     PerssonAVMethod(c_av=0.1, av_form="element_local_DD" if av == "local_dd" else "conservative_br0"))
+                s = GpuSolve(st, Euler2D(1.4), m, ctx=ctx)
+                s.upload(st.u, 0.0)
+                best, _ = s.autotune(reps=reps)
+                out[f"p{p}_{flux}_{av}"] = int(best)
+                s.close()
+    save(path)
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="measure the tile table on this GPU and save it as JSON")
+    ap.add_argument("--out", default=DEFAULT_TABLE)
+    a = ap.parse_args()
+    print(json.dumps(measure(a.out)))
