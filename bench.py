@@ -714,10 +714,12 @@ def run_ncu_target(args):
                    C3.cfl, C3.steps, seed=C3.seed, jump_scale=C3.jump_scale)
     st, method = w.build(F)
     solve = F.GpuSolve(st, F.Euler2D(1.4), method)
+    if args.variant is not None:
+        solve.set_variant(args.variant)
     solve.upload(st.u, 0.0)
     ms, r = solve.time_stages(args.steps, cfl=C3.cfl)
-    print(json.dumps({"ncu_target": True, "n": args.n, "steps": args.steps, "stage_ms": [float(x) for x in ms],
-                      "status": r["status"]}))
+    print(json.dumps({"ncu_target": True, "n": args.n, "steps": args.steps, "variant": solve.variant()[0],
+                      "stage_ms": [float(x) for x in ms], "status": r["status"]}))
     return 0
 
 
@@ -732,6 +734,8 @@ def main():
     ap.add_argument("--served-requests", type=int, default=32)
     ap.add_argument("--ncu-target", action="store_true")
     ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--variant", type=int, default=None,
+                    help="--ncu-target: tile variant of the stage kernel (default: variant 0)")
     ap.add_argument("--flux", choices=["hllc", "rusanov"], default=None,
                     help="--ncu-target: numerical flux (default: the workload's, HLLC)")
     ap.add_argument("--method", choices=["persson_av", "null"], default=None,

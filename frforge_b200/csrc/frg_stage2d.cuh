@@ -322,9 +322,10 @@ FRG_DEV void tile_compute(const OpsT<NP>& ops, const Mesh2Dev& M, const Phys& P,
 
   if (!prime) {
     // ------------------------------------------------------- P1 fluxes
-    // item = o + NOWN*k: lanes walk over elements
+    // item = k + NP2*o: lanes walk over the points of an element, so a warp's
+    // loads of the staged state are consecutive words (no bank conflicts)
     for (int idx = tid; idx < NOWN * NP2; idx += NT) {
-      const int o = idx % NOWN, k = idx / NOWN;
+      const int k = idx % NP2, o = idx / NP2;
       const int s = (o / TX + 1) * BX + (o % TX) + 1;
       if (!INT && (!(sFlag[s] & kSlotOwn) || (sFlag[s] & kSlotSolid))) continue;
       double U[4], F[4], G[4];
