@@ -8,7 +8,9 @@ evaluations over all 512^2 x 16 x 4 = 16.8M degrees of freedom.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --workload batched     # 64 mixed solves, batched vs one at a time
   python bench.py --workload served      # Poisson request trace, served vs one at a time
-  python bench.py --ncu-target [--n 256] # a few stage launches of the workload, for ncu
+  python bench.py --workload c1          # the 1D 256-element case (launch-bound), steps/s
+  python bench.py --ncu-target [--n 256] [--variant V] [--flux F] [--method M]
+                                         # a few stage launches of the workload, for ncu
 
 ours: value = DOF-stage/s with the state resident in HBM, timed with CUDA
 events on the library's stream (max over ranks); e2e = the same metric through
@@ -18,6 +20,8 @@ around every stage launch; cpu_baseline = the C oracle on a bounded sample.
 reference: the reference algorithm on the host cores (the C oracle port, all
 threads), each step one full SSP-RK3 step of the 512^2 workload.
 Multi-GPU: replicas only (each rank runs its own solve, no data exchange).
+The batched and served arms start from the committed B200 tile table
+(frforge_b200/autotune_b200.json; --no-tune: default tiles).
 """
 from __future__ import annotations
 
