@@ -296,10 +296,14 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
       bad_du |= !isfinite(du);
       bad_u |= !isfinite(un);
     }
-    const int any_du = __syncthreads_or(bad_du);
-    const int any_u = __syncthreads_or(bad_u);
-    if (tid == 0 && (any_du || any_u) && B.sc)
-      atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
+    // one barrier that also votes on non-finite values; only a tile with one
+    // tells the residual and the state apart
+    if (__syncthreads_or(bad_du | bad_u)) {
+      const int any_du = __syncthreads_or(bad_du);
+      const int any_u = __syncthreads_or(bad_u);
+      if (tid == 0 && B.sc)
+        atomicOr(&B.sc->flags, ((any_du ? 1u : 0u) | (any_u ? 2u : 0u)) << (2 * (B.stage - 1)));
+    }
     if (B.mode == kModeResidual) return;
   } else {
     for (int idx = tid; idx < TX * NEQ * NP; idx += nthr) {
