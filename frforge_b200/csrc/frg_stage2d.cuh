@@ -960,11 +960,18 @@ __device__ __forceinline__ void stage2d_tile(const OpsT<NP>& ops, const Mesh2Dev
   using S = Smem2D<NP, TX, TY, U0S, MINB, NTHR>;
   extern __shared__ __align__(16) double smem[];
   StageCtl ctl;
-  if (!stage_control(B, ctl)) return;
+  ctl.prime = (B.mode == kModePrime) || (B.mode == kModeSense);
+  ctl.need_u0 = (B.mode == kModeStage) && (B.stage != 1);
   const TileBuf tb = tile_buf<S>(smem);
   tile_slots<S>(M, tb, tx0, ty0, ctl.prime);
   __syncthreads();
+  // the copies go out before the step's status is read, so that the status
+  // load overlaps them; a skipped stage waits for its copies and writes nothing
   tile_issue<NP, AV, S, PRE>(M, B, tb, ctl);
+  if (!stage_control(B, ctl)) {
+    cp_async_wait<0>();
+    return;
+  }
   // interior tiles of P >= 4 (NP >= 5) run the general body: the interior
   // body does not fit their 64 registers per thread and spills (measured on
   // a B200: P = 4 and 5 are 11-17 % faster without it, P = 1..3 11-21 %
