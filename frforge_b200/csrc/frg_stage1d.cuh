@@ -63,17 +63,21 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
   const int nel = M.nel;
   const size_t cs = (size_t)nel * NP;
 
-  double dt = 0.0, tstage = 0.0;
+  // the step's status words are loaded first and tested after the staging
+  // below, so that their latency overlaps the staging loads; a skipped stage
+  // has written nothing when it returns
+  int sc_active = 1;
+  unsigned sc_flags = 0u;
+  double dt = 0.0, tstage = 0.0, sc_t0 = 0.0;
   if (B.use_sc) {
-    if (!B.sc->active || (B.sc->flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
+    sc_active = B.sc->active;
+    sc_flags = B.sc->flags;
     dt = B.sc->dt;
-    const double t0 = B.sc->t0;
-    tstage = (B.stage == 1) ? t0 : (B.stage == 2 ? t0 + dt : t0 + dt / 2.0);
+    sc_t0 = B.sc->t0;
   } else if (B.sc) {
     tstage = B.sc->t;
     dt = B.sc->dt;
   }
-  (void)tstage;
   const bool prime = (B.mode == kModePrime) || (B.mode == kModeSense);
 
   for (int s = tid; s < NSLOT; s += nthr) {
@@ -109,6 +113,11 @@ __device__ __forceinline__ void stage1d_tile(const OpsT<NP>& ops, const Mesh1Dev
     }
   }
   __syncthreads();
+  if (B.use_sc) {
+    if (!sc_active || (sc_flags & (B.stage == 1 ? 0u : (B.stage == 2 ? 1u : 5u)))) return;
+    tstage = (B.stage == 1) ? sc_t0 : (B.stage == 2 ? sc_t0 + dt : sc_t0 + dt / 2.0);
+  }
+  (void)tstage;
 
   // extrapolate_interface override (residual!, Residual.jl:175): both traces
   // of every staged element, for the numerical fluxes; the BR0 terms keep
