@@ -86,10 +86,13 @@ __global__ void __launch_bounds__(NTHR, MINB)
   static_assert(sizeof(Mesh2Dev) + sizeof(Phys) + sizeof(StageBufs) + 64 <= kBatchStaticSmem, "static smem");
   const BatchTile t = tiles[blockIdx.x];
   const BatchInst* I = &insts[t.inst];
-  if (mode == kModeStage && stage == 3 && I->rk2) return;  // SSP-RK2 has two stages
-  if (mode == kModePrime && !I->sc->stepped_ok) return;    // post-step pass: completed steps only
+  // the descriptor copies go out first; the instance's skip tests, whose
+  // loads overlap them, come after (a skipped CTA has written nothing)
   copy_to_smem(&sM, &I->M2);
   copy_to_smem(&sP, &I->P);
+  if ((mode == kModeStage && stage == 3 && I->rk2) ||     // SSP-RK2 has two stages
+      (mode == kModePrime && !I->sc->stepped_ok))          // post-step pass: completed steps only
+    return;
   if (threadIdx.x == 0) sB = batch_bufs(*I, stage, mode);
   __syncthreads();
   stage2d_tile<NP, FLUX, AV, TX, TY, MINB, U0S, NTHR>(ops, sM, sP, sB, t.x0, t.y0);
@@ -104,10 +107,9 @@ __global__ void __launch_bounds__(256)
   __shared__ __align__(16) StageBufs sB;
   const BatchTile t = tiles[blockIdx.x];
   const BatchInst* I = &insts[t.inst];
-  if (mode == kModeStage && stage == 3 && I->rk2) return;
-  if (mode == kModePrime && !I->sc->stepped_ok) return;
   copy_to_smem(&sM, &I->M1);
   copy_to_smem(&sP, &I->P);
+  if ((mode == kModeStage && stage == 3 && I->rk2) || (mode == kModePrime && !I->sc->stepped_ok)) return;
   if (threadIdx.x == 0) sB = batch_bufs(*I, stage, mode);
   __syncthreads();
   stage1d_tile<NP, FLUX, AV>(ops, sM, sP, sB, t.x0);
